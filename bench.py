@@ -1,0 +1,353 @@
+#!/usr/bin/env python
+"""Headline benchmark: all-pairs vortex-particle interaction driven by RK4.
+
+Workload: the leapfrogging coaxial ring pair, N = 131,072 (2 wakes x 8,192
+stations x 8 core particles), nu = 1e-4 with PSE diffusion, dt = 0.005; FP32
+pair math with FP64 accumulation, FP64 RK4 state.  One step = one RK4 step =
+4 right-hand sides = 4 N^2 pair interactions (the N-body convention; the
+reference's symmetric loop evaluates N(N-1)/2 kernels per RHS for the same
+credit).  Seeded synthetic geometry (no dataset exists for this path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pawan|reference]
+
+Prints one JSON line (rank 0).  `value` is device-timed throughput with the
+state resident in HBM; `e2e` is the same metric through the C ABI with host
+buffers (state H2D and D2H every step); `roofline` is the FP32 pair kernel's
+algorithmic flop rate (96 flops per interaction with diffusion) against the
+FP32 FFMA throughput measured in the same run; `cpu_baseline` is the
+reference's own OpenMP __parallel::solve (compiled from its sources) on a
+bounded sample, on this host's cores.  With --gpus N (torchrun), every rank
+runs its own ring pair (independent replicas, weak scaling); the time is the
+max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FLOPS_NU = 96      # algorithmic flops per interaction with diffusion
+FLOPS_NO_NU = 79   # without (nu = 0)
+METRIC = "G pair-interactions/s at N=131k vs plain FP64 GPU; batched solves/s, p99 latency"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["pawan", "reference"], default="pawan")
+    ap.add_argument("--n-stations", type=int, default=8192, help="stations per ring (8 particles each)")
+    ap.add_argument("--quick", action="store_true",
+                    help="main timed loop only (no autotune, FP64 comparison, e2e, CPU baseline)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ ranks
+
+class Ranks:
+    def __init__(self, gpus: int):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.dist = None
+        if self.world > 1:
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", self.local))
+            self.dist = dist
+            self.torch = torch
+
+    def barrier(self):
+        if self.dist:
+            self.dist.barrier()
+
+    def max(self, v: float) -> float:
+        if not self.dist:
+            return v
+        t = self.torch.tensor([v], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.dist:
+            self.dist.destroy_process_group()
+
+
+# ----------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.tmp = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.tmp, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.tmp.flush()
+        rows = []
+        with open(self.tmp.name) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.unlink(self.tmp.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
+
+
+def gpu_index(local: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    parts = [p for p in vis.split(",") if p.strip()]
+    if parts and parts[min(local, len(parts) - 1)].strip().isdigit():
+        return int(parts[min(local, len(parts) - 1)])
+    return local
+
+
+def traffic_from_profiles():
+    """DRAM bytes per pair launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "pair_f32_ring_pair.json")
+    if os.path.exists(p):
+        try:
+            d = json.load(open(p))
+            return d.get("dram_bytes_per_launch_full_size")
+        except (OSError, ValueError):
+            return None
+    return None
+
+
+# ------------------------------------------------------------ CPU baseline
+
+def cpu_reference_sample(pos, vor, rad, vol, nu, target_s: float, cap_n: int = 16384):
+    """Times the reference's OpenMP __parallel::solve() on the first n particles
+    of the workload, growing n until one solve takes about target_s seconds.
+    Returns (interactions per second, n, seconds, threads)."""
+    import oracle
+    threads = oracle.ref_max_threads()
+    n = 1024
+    while True:
+        ref = oracle.RefSystem([n], pos[:n], vor[:n], rad[:n], vol[:n], nu, parallel=True)
+        t0 = oracle.ref_wtime()
+        ref.solve()
+        dt = oracle.ref_wtime() - t0
+        ref.close()
+        if dt >= target_s or n >= cap_n:
+            return n * n / dt, n, dt, threads
+        grow = max(1.25, min(2.0, (target_s / max(dt, 1e-3)) ** 0.5))
+        n = min(cap_n, int(n * grow) // 8 * 8)
+
+
+def run_reference(args, rk: Ranks):
+    from pawan_b200 import geometry as g
+    if rk.rank != 0:
+        return
+    sc = g.ring_pair(n_stations=args.n_stations, steps=1)
+    pos, vor, rad, vol = sc.union()
+    per_step = max(1.0, min(5.0, 150.0 / max(1, args.steps + args.warmup)))
+    rate, n, dt, threads = cpu_reference_sample(pos, vor, rad, vol, sc.nu, per_step)
+    import oracle
+    for _ in range(args.warmup):
+        ref = oracle.RefSystem([n], pos[:n], vor[:n], rad[:n], vol[:n], sc.nu, parallel=True)
+        ref.solve()
+        ref.close()
+    times = []
+    for _ in range(args.steps):
+        ref = oracle.RefSystem([n], pos[:n], vor[:n], rad[:n], vol[:n], sc.nu, parallel=True)
+        t0 = oracle.ref_wtime()
+        ref.solve()
+        times.append(oracle.ref_wtime() - t0)
+        ref.close()
+    tot = sum(times)
+    value = args.steps * n * n / tot / 1e9
+    sample = (f"one __parallel::solve() (reference OpenMP path, compiled from its sources) per step "
+              f"on the first {n} particles of the ring pair; {threads} threads")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "G interactions/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ring pair geometry)",
+            "config": {"workload": f"ring_pair N={sc.n} (sampled to {n} particles on CPU)",
+                       "n_particles": sc.n, "sample_particles": n, "nu": sc.nu},
+            "cpu_baseline": {"value": value, "unit": "G interactions/s", "cores": threads,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "G interactions/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- GPU arm
+
+def run_pawan(args, rk: Ranks):
+    import pawan_b200
+    from pawan_b200 import Context, System
+    from pawan_b200 import geometry as g
+
+    sc = g.ring_pair(n_stations=args.n_stations, steps=1)
+    N = sc.n
+    pos, vor, rad, vol = sc.union()
+    dt = sc.dt
+    flops = FLOPS_NU if sc.nu != 0 else FLOPS_NO_NU
+    ctx = Context(rk.local)
+    info = ctx.info()
+    s = System.from_scenario(ctx, sc, "f32")
+    tuned = s.get_config() if args.quick else s.autotune()
+
+    for _ in range(args.warmup):
+        s.rk4(dt, 1)
+        ctx.flush_l2()
+    ctx.synchronize()
+
+    rk.barrier()
+    ctx.synchronize()
+    clocks = ClockSampler(gpu_index(rk.local))
+    clocks.start()
+    ctx.profile(True)
+    launches0 = ctx.launch_count
+    ctx.mark(0)
+    for _ in range(args.steps):
+        s.rk4(dt, 1)
+        ctx.flush_l2()  # evicts L2 between timed steps (256 MiB write, <0.1% of a step)
+    ctx.mark(1)
+    ms = ctx.elapsed_ms(0, 1)
+    ctx.synchronize()
+    launches = ctx.launch_count - launches0
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    clk = clocks.stop()
+    rk.barrier()
+    ms_max = rk.max(ms)
+    total_inter = rk.world * 4.0 * N * N * args.steps
+    value = total_inter / (ms_max * 1e-3) / 1e9
+
+    pair_avg_s = prof["pair_ms"] / max(1, prof["pair_launches"]) * 1e-3
+    achieved_tflops = N * N * flops / pair_avg_s / 1e12
+    peak_tflops = ctx.peak_fp32(2.0) / 1e3
+    state = s.get_states()
+    assert np.all(np.isfinite(state)), "non-finite state"
+
+    line = {"metric": METRIC, "value": value, "unit": "G interactions/s", "n_gpus": rk.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded ring pair geometry, jitter 1e-4)",
+            "config": {"workload": f"leapfrogging coaxial ring pair, N={N}, nu={sc.nu}, dt={dt}, RK4 step",
+                       "n_particles": N, "wakes": len(sc.counts), "precision": "fp32 pairs, fp64 accumulation+state",
+                       "parallelism": f"replicas x{rk.world}", "l2": "flushed between timed steps (256 MiB write)",
+                       "tile": tuned, "sm_count": info["sm_count"]},
+            "gpu_launches": int(launches), "clocks": clk,
+            "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": peak_tflops,
+                         "unit": "TFLOP/s", "frac": achieved_tflops / peak_tflops,
+                         "traffic": traffic_from_profiles(),
+                         "kernel": "pairs_f32_kernel", "flops_per_interaction": flops,
+                         "pair_launch_ms": pair_avg_s * 1e3,
+                         "peak_source": "measured: FFMA-chain probe (pawan_peak_fp32) in this run"}}
+
+    if not args.quick:
+        # plain FP64 comparator and tuned FP64 on the same workload: one RHS each
+        cmp = {}
+        for prec in ("f64_plain", "f64"):
+            s64 = System.from_scenario(ctx, sc, prec)
+            s64.solve()
+            ctx.synchronize()
+            ctx.profile(True)
+            s64.solve()
+            p64 = ctx.profile_read()
+            ctx.profile(False)
+            t = p64["pair_ms"] * 1e-3
+            cmp[prec] = {"value": N * N / t / 1e9, "unit": "G interactions/s", "pair_launch_ms": t * 1e3}
+            s64.close()
+        f32_rate = N * N / pair_avg_s / 1e9
+        line["vs_plain_fp64"] = {"fp32_pair_rate": f32_rate, "fp64_plain": cmp["f64_plain"],
+                                 "fp64_tuned": cmp["f64"],
+                                 "speedup_vs_plain": f32_rate / cmp["f64_plain"]["value"],
+                                 "speedup_vs_tuned_fp64": f32_rate / cmp["f64"]["value"]}
+        line["peak_fp64_tflops"] = ctx.peak_fp64(1.0) / 1e3
+
+        # end to end through the C ABI: pinned host state in, RK4 step, state out
+        hin = ctx.pinned((6 * N,))
+        hout = ctx.pinned((6 * N,))
+        hin[:] = sc.state()
+        s.set_states(hin)
+        s.rk4(dt, 1)
+        s.get_states(hout)
+        rk.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            s.set_states(hin)
+            s.rk4(dt, 1)
+            s.get_states(hout)
+        t_e2e = rk.max(time.perf_counter() - t0)
+        line["e2e"] = {"value": rk.world * 4.0 * N * N * args.steps / t_e2e / 1e9, "unit": "G interactions/s",
+                       "h2d_bytes_per_step": int(hin.nbytes), "d2h_bytes_per_step": int(hout.nbytes),
+                       "path": "pawan_system_set_states (pinned host) -> pawan_system_rk4 -> pawan_system_get_states"}
+
+        if rk.rank == 0 and rk.world == 1 and not args.no_cpu_baseline:
+            try:
+                rate, n, tsec, threads = cpu_reference_sample(pos, vor, rad, vol, sc.nu, 10.0)
+                line["cpu_baseline"] = {
+                    "value": rate / 1e9, "unit": "G interactions/s", "cores": threads, "kind": "reference",
+                    "sample": f"one __parallel::solve() of the reference (OpenMP, compiled from its sources) "
+                              f"on the first {n} particles of the ring pair, {tsec:.1f} s"}
+            except Exception as e:  # the reference build may be absent on a fresh checkout
+                line["cpu_baseline"] = {"value": None, "unit": "G interactions/s", "cores": 0,
+                                        "kind": "reference", "sample": f"unavailable: {e}"}
+    s.close()
+    ctx.close()
+    if rk.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rk = Ranks(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rk)
+        else:
+            run_pawan(args, rk)
+    finally:
+        rk.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,216 @@
+/* pawan_b200 -- C ABI of the B200 (sm_100a) implementation of pawan's hot
+ * path: the all-pairs vortex-particle interaction and the RK4 integration
+ * that drives it.
+ *
+ * Plain C types only (pointers, sizes, doubles); no CUDA or C++ types cross
+ * this boundary.  Every call returns a status (PAWAN_OK == 0); the text of the
+ * last failure on a context is pawan_ctx_last_error().  No C++ exception
+ * crosses the ABI.  Host pointers are borrowed for the duration of the call
+ * only.  A context is used from one host thread at a time (the serving
+ * engine runs its own worker thread on a context it owns).
+ *
+ * Layout conventions (the reference's, src/wake/wake.cpp:87-120):
+ *   - a system's particles are the union of its wakes in wake order;
+ *   - position / vorticity arrays are N x 3 row-major doubles;
+ *   - a state or rate vector has size 6*N ("_size", src/system/system.h:22)
+ *     and holds, per wake, [x (N_w x 3) | alpha (N_w x 3)], wakes concatenated
+ *     (src/interaction/interaction.cpp:204-229).
+ *
+ * Each entry point names the reference interface it replaces.
+ */
+#ifndef PAWAN_B200_H
+#define PAWAN_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define PAWAN_OK 0
+#define PAWAN_ERR_INVALID 1     /* bad argument, size or handle */
+#define PAWAN_ERR_CUDA 2        /* CUDA runtime error (text in last_error) */
+#define PAWAN_ERR_NOMEM 3       /* device or host allocation failed */
+#define PAWAN_ERR_STATE 4       /* call not valid in the object's state */
+#define PAWAN_ERR_BUDGET 5      /* serving: request can never fit the budget */
+#define PAWAN_ERR_TIMEOUT 6     /* serving: wait ran out */
+#define PAWAN_ERR_NOTFOUND 7    /* serving: unknown request id */
+#define PAWAN_ERR_REJECTED 8    /* serving: queue full or engine stopped */
+
+/* ---------------------------------------------------------- pair precision */
+#define PAWAN_PREC_F32 0        /* FP32 pair math, FP64 per-tile accumulation */
+#define PAWAN_PREC_F64 1        /* FP64, same algebra as the FP32 kernel */
+#define PAWAN_PREC_F64_PLAIN 2  /* FP64, the reference's formula term by term */
+
+typedef struct pawan_ctx pawan_ctx;
+typedef struct pawan_system pawan_system;
+typedef struct pawan_batch pawan_batch;
+typedef struct pawan_server pawan_server;
+
+/* ---------------------------------------------------------------- context */
+/* One device, one stream.  No reference counterpart: the reference has no
+ * device state. */
+int pawan_ctx_create(int device, pawan_ctx **out);
+void pawan_ctx_destroy(pawan_ctx *ctx);
+const char *pawan_ctx_last_error(const pawan_ctx *ctx);
+const char *pawan_status_name(int status);
+/* sm_count, compute capability, total device memory in bytes. */
+int pawan_ctx_info(pawan_ctx *ctx, int *sm_count, int *cc_major, int *cc_minor,
+                   size_t *total_mem);
+int pawan_ctx_synchronize(pawan_ctx *ctx);
+/* Number of this library's kernels launched on the context so far. */
+unsigned long long pawan_ctx_launch_count(const pawan_ctx *ctx);
+/* Time every pair-kernel launch with CUDA events on the launching stream. */
+int pawan_ctx_profile(pawan_ctx *ctx, int enable);
+/* Totals since profiling was (re)enabled: summed pair-kernel time (ms),
+ * pair launches, and pair interactions counted as N^2 per solve per launch. */
+int pawan_ctx_profile_read(pawan_ctx *ctx, double *pair_ms, unsigned long long *pair_launches,
+                           double *pair_interactions);
+/* Timing marks on the context's stream (CUDA events, slots 0..15) and the
+ * device time between two of them, in ms (waits for the later mark). */
+int pawan_ctx_mark(pawan_ctx *ctx, int slot);
+int pawan_ctx_elapsed(pawan_ctx *ctx, int slot0, int slot1, double *ms);
+/* Overwrites `bytes` of device scratch on the context's stream, evicting the
+ * L2 cache between timed iterations. */
+int pawan_ctx_flush_l2(pawan_ctx *ctx, size_t bytes);
+/* Pinned host memory (for host<->device copies at full bandwidth). */
+int pawan_host_alloc(pawan_ctx *ctx, size_t bytes, void **out);
+int pawan_host_free(pawan_ctx *ctx, void *ptr);
+
+/* ----------------------------------------------------------------- system */
+/* A system is the reference's __interaction (src/interaction/interaction.h:21-235)
+ * with its wakes: all-pairs over the union of the wakes, viscosity nu.
+ * Replaces __interaction(W) / __interaction(W1,W2) / addWake
+ * (interaction.cpp:11-39) and __parallel(W), __parallel(W1,W2)
+ * (src/interaction/parallel.cpp:10-11).  The reference hard-codes
+ * nu = 2.5e-3 (interaction.cpp:13); here it is an argument. */
+int pawan_system_create(pawan_ctx *ctx, size_t n_wakes, const size_t *num_particles, double nu,
+                        int precision, pawan_system **out);
+void pawan_system_destroy(pawan_system *sys);
+/* __system::_size (src/system/system.h:22): 6 * total particles. */
+size_t pawan_system_size(const pawan_system *sys);
+size_t pawan_system_num_particles(const pawan_system *sys);
+/* Particle data of all wakes (union, N x 3 / N): the fields of __wake
+ * (src/wake/wake.h:35-41) that the interaction reads. */
+int pawan_system_set_particles(pawan_system *sys, const double *position, const double *vorticity,
+                               const double *radius, const double *volume);
+/* __interaction::setStates / getStates (interaction.cpp:204-211, 222-229). */
+int pawan_system_set_states(pawan_system *sys, const double *state, size_t size);
+int pawan_system_get_states(pawan_system *sys, double *state, size_t size);
+/* __interaction::solve -> interact() (interaction.cpp:41-43, 95-108) and
+ * __parallel::interact (parallel.cpp:13-85): velocity and vorticity rate of
+ * every particle.  Asynchronous; read the result with get_rates. */
+int pawan_system_solve(pawan_system *sys);
+/* __interaction::getRates (interaction.cpp:213-220): [u | dalpha] per wake. */
+int pawan_system_get_rates(pawan_system *sys, double *rate, size_t size);
+/* W->_velocity and W->_retvorcity of one wake (N_w x 3 each; wake.h:36,38). */
+int pawan_system_get_wake_rates(pawan_system *sys, size_t wake, double *velocity,
+                                double *retvorcity);
+/* nsteps of __rk4::step (src/integration/rk4.cpp:12-76), state kept on the
+ * device between steps; read it back with get_states. */
+int pawan_system_rk4(pawan_system *sys, double dt, size_t nsteps);
+/* nsteps of __integration::step (src/integration/integration.cpp:37-45). */
+int pawan_system_euler(pawan_system *sys, double dt, size_t nsteps);
+/* __interaction::diagnose (interaction.cpp:49-93), FP64 on the device.
+ * out[0..2] total vorticity, [3..5] linear impulse, [6..8] angular impulse,
+ * [9] enstrophy, [10] helicity.  quadratic = 0 skips the O(N^2) terms
+ * (out[9], out[10] then 0). */
+int pawan_system_diagnose(pawan_system *sys, double *out, int quadratic);
+/* calculateKineticEnergy over all wakes (interaction.cpp:351-383). */
+int pawan_system_kinetic_energy(pawan_system *sys, double *ke);
+/* The protected __interaction::_nu (interaction.h:24). */
+int pawan_system_set_nu(pawan_system *sys, double nu);
+int pawan_system_set_precision(pawan_system *sys, int precision);
+/* Appends (append != 0) or writes one .wake frame: t (f64), nWake (size_t),
+ * then per wake N (size_t), position (N x 3 f64), vorticity (N x 3 f64),
+ * radius (N f64): __integration::integrate's per-step output
+ * (integration.cpp:20-21, 28-29; interaction.cpp:197-202; wake.cpp:68-73). */
+int pawan_system_write_frame(pawan_system *sys, const char *path, double t, int append);
+/* Pair-kernel tiling: threads per block, threads per target, unroll depth,
+ * work items per SM slot.  set_config fixes it; autotune measures the
+ * candidates on this system and keeps the fastest. */
+int pawan_system_set_config(pawan_system *sys, int threads, int threads_per_target, int unroll,
+                            int items_per_slot);
+int pawan_system_get_config(pawan_system *sys, int *threads, int *threads_per_target,
+                            int *unroll, int *items_per_slot);
+int pawan_system_autotune(pawan_system *sys);
+/* Device address of the state [x | alpha] in union layout (6N doubles,
+ * x = first 3N) for callers that keep data on the device. */
+int pawan_system_device_state(pawan_system *sys, double **state);
+
+/* ------------------------------------------------------------------ batch */
+/* Many independent systems in one persistent pair launch per RK4 stage
+ * (ragged segments), the four stages optionally captured in a CUDA graph.
+ * No reference counterpart (the reference integrates one system at a time).
+ * Each system's result matches its own pawan_system_rk4 result up to the
+ * FP64 rounding of how its source chunks are grouped; graph and non-graph
+ * runs of one batch agree bit for bit. */
+int pawan_batch_create(pawan_ctx *ctx, size_t n, pawan_system *const *systems, pawan_batch **out);
+void pawan_batch_destroy(pawan_batch *batch);
+/* dt[i] for system i (NULL: every system uses dt0). */
+int pawan_batch_rk4(pawan_batch *batch, const double *dt, double dt0, size_t nsteps,
+                    int use_graph);
+int pawan_batch_solve(pawan_batch *batch);
+int pawan_batch_set_config(pawan_batch *batch, int threads, int threads_per_target, int unroll,
+                           int items_per_slot);
+int pawan_batch_autotune(pawan_batch *batch);
+
+/* ---------------------------------------------------------------- serving */
+/* A request loop with device-resident state and continuous batching: each
+ * engine iteration advances every admitted request by one RK4 step in one
+ * batched launch sequence; requests that arrive meanwhile are admitted when
+ * the HBM budget and the per-iteration work cap allow.  No reference
+ * counterpart. */
+typedef struct {
+  double budget_bytes;          /* device memory the admitted requests may hold */
+  double max_step_interactions; /* cap on sum N^2 of the requests in one iteration (0: none) */
+  int max_active;               /* cap on admitted requests (0: none) */
+  int max_queue;                /* waiting requests beyond this are rejected (0: none) */
+  int precision;                /* PAWAN_PREC_* */
+} pawan_serve_config;
+
+typedef struct {
+  unsigned long long submitted, admitted, completed, rejected, queued, active;
+  unsigned long long iterations;
+  double interactions;          /* pair interactions computed (N^2 per solve per RHS) */
+  double busy_seconds;          /* wall time the engine spent in iterations */
+  double bytes_in_use;
+} pawan_serve_stats;
+
+#define PAWAN_REQ_QUEUED 0
+#define PAWAN_REQ_ACTIVE 1
+#define PAWAN_REQ_DONE 2
+#define PAWAN_REQ_REJECTED 3
+#define PAWAN_REQ_CANCELLED 4
+
+int pawan_server_create(pawan_ctx *ctx, const pawan_serve_config *cfg, pawan_server **out);
+/* Stops the worker (in-flight iteration finishes) and frees everything. */
+void pawan_server_destroy(pawan_server *srv);
+/* Copies the request's particles; returns its id.  nsteps RK4 steps of dt. */
+int pawan_server_submit(pawan_server *srv, size_t n_wakes, const size_t *num_particles,
+                        const double *position, const double *vorticity, const double *radius,
+                        const double *volume, double nu, double dt, size_t nsteps,
+                        long long *id);
+int pawan_server_poll(pawan_server *srv, long long id, int *state);
+/* Blocks until the request is done, rejected or cancelled, or timeout_s passes. */
+int pawan_server_wait(pawan_server *srv, long long id, double timeout_s);
+/* Final state (reference layout, 6N) and timing of a finished request; the
+ * request is forgotten afterwards.  Times are seconds since the server was
+ * created. */
+int pawan_server_fetch(pawan_server *srv, long long id, double *state, size_t size,
+                       double *t_submit, double *t_admit, double *t_done);
+int pawan_server_cancel(pawan_server *srv, long long id);
+int pawan_server_stats(pawan_server *srv, pawan_serve_stats *out);
+
+/* ----------------------------------------------------- throughput probes */
+/* Measured FP32 FFMA / FP64 DFMA throughput of the device, GFLOP/s (FMA = 2
+ * flops), over `seconds` of back-to-back probe launches. */
+int pawan_peak_fp32(pawan_ctx *ctx, double seconds, double *gflops);
+int pawan_peak_fp64(pawan_ctx *ctx, double seconds, double *gflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PAWAN_B200_H */

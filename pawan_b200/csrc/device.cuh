@@ -1,0 +1,90 @@
+// Shared device-side types of the pawan B200 library.
+//
+// HBM layout of one system (the reference's __interaction over its wakes,
+// src/interaction/interaction.h:21-235), all particles of all wakes in wake
+// order, N in total:
+//   X      double[6N]  state [x (N x 3) | alpha (N x 3)]  (the reference keeps
+//                      this per wake, wake.cpp:87-120; the host API converts)
+//   rad    double[N]   smoothing radius s          (wake.h:39)
+//   vol    double[N]   particle volume v           (wake.h:40)
+//   pos32  float4[N]   (x, y, z, s^2/2)   packed FP32 source/target tile data
+//   vor32  float4[N]   (ax, ay, az, v)    32 bytes per particle in total
+//   pos64  double4[N]  (x, y, z, s)       packed FP64 data (FP64 kernels)
+//   vor64  double4[N]  (ax, ay, az, v)
+//   partial double[C][6][N]  per source-chunk sums (u, dalpha) of the pair
+//                      kernel, reduced in fixed chunk order by the stage kernel
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pawan {
+
+// One solve as the pair kernels see it.
+struct SegDesc {
+  const float4 *pos32;
+  const float4 *vor32;
+  const double4 *pos64;
+  const double4 *vor64;
+  double *partial;  // [nchunks][6][n]
+  int n;
+  int nchunks;
+  double nu;
+};
+
+// One unit of pair work: targets [t0, t0 + targets_per_block) of segment `seg`
+// against its sources [s0, s1), written to partial chunk `chunk`.
+struct WorkItem {
+  int seg;
+  int t0;
+  int chunk;
+  int s0;
+  int s1;
+};
+
+// One block of the per-particle stage kernel: particles [l0, l0 + 256) of
+// segment `seg`.
+struct StageItem {
+  int seg;
+  int l0;
+};
+
+// What the stage kernel needs of one segment.
+struct StageDesc {
+  const double *partial;
+  int nchunks;
+  int n;
+  double *X;   // state x
+  double *Xs;  // stage state x_s
+  double *K1;  // k1
+  double *K2;  // k2, then k2 + k3
+  double *R;   // rates of a plain solve
+  const double *rad;
+  const double *vol;
+  float4 *pos32;
+  float4 *vor32;
+  double4 *pos64;
+  double4 *vor64;
+  double dt;
+};
+
+enum StageMode : int {
+  STAGE_RATES = 0,   // R = sum of partials
+  STAGE_K1 = 1,      // k1 = r; x_s = k1*(dt/2) + x; pack x_s
+  STAGE_K2 = 2,      // k2 = r; x_s = k2*(dt/2) + x; pack x_s
+  STAGE_K3 = 3,      // k2 = k2 + r; x_s = r*dt + x; pack x_s
+  STAGE_FINAL = 4,   // x = x + ((k1 + r)*(dt/6) + (k2+k3)*(dt/3)); pack x
+  STAGE_EULER = 5,   // x = x + r*dt; pack x   (integration.cpp:37-45)
+  STAGE_PACK = 6,    // pack x only
+};
+
+enum PackFlags : int { PACK_F32 = 1, PACK_F64 = 2 };
+
+// 1/(4 pi) and friends.
+constexpr double kInv4Pi = 0.07957747154594766788;
+constexpr double kInvPi = 0.31830988618379067154;
+
+// Block sizes.
+constexpr int kStageThreads = 256;
+
+}  // namespace pawan

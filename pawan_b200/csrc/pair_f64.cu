@@ -1,0 +1,165 @@
+// All-pairs interaction in FP64 with the algebra of the FP32 kernel
+// (pair_f32.cu): two rsqrt per pair, no pow, no division.  This is the
+// "tuned FP64" variant, reported beside the FP32 kernel and the plain FP64
+// comparator (pair_plain.cu).  Same work items, partial layout and gather form.
+//
+// Reference: INTERACT (src/interaction/interaction_utils.h:363-407), KERNEL
+// (src/interaction/highorder.h:48-60), __interaction::interact
+// (src/interaction/interaction.cpp:95-108).
+#include "device.cuh"
+#include "kernels.h"
+
+namespace pawan {
+namespace {
+
+__device__ __forceinline__ void load_source_f64(const SegDesc &sg, int j, int s1, double4 &p,
+                                                double4 &v) {
+  if (j < s1) {
+    p = sg.pos64[j];
+    v = sg.vor64[j];
+  } else {
+    p = make_double4(1e150, 1e150, 1e150, 1.0);
+    v = make_double4(0.0, 0.0, 0.0, 0.0);
+  }
+}
+
+template <int TB, bool DIFF>
+__global__ void __launch_bounds__(TB)
+    pairs_f64_kernel(const WorkItem *__restrict__ items, int n_items,
+                     const SegDesc *__restrict__ segs, int *__restrict__ next_item) {
+  __shared__ double4 sp[2][TB];
+  __shared__ double4 sv[2][TB];
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(next_item, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= n_items) break;
+
+    const WorkItem w = items[it];
+    const SegDesc sg = segs[w.seg];
+    const int i = w.t0 + tid;
+    const bool valid = i < sg.n;
+    double4 pi = make_double4(0.0, 0.0, 0.0, 1.0);
+    double4 vi = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (valid) {
+      pi = sg.pos64[i];
+      vi = sg.vor64[i];
+    }
+    const double hi = 0.5 * pi.w * pi.w;
+    double ux = 0, uy = 0, uz = 0, qx = 0, qy = 0, qz = 0, gx = 0, gy = 0, gz = 0;
+    double ex = 0, ey = 0, ez = 0, ev = 0;
+
+    const int ntiles = (w.s1 - w.s0 + TB - 1) / TB;
+    double4 rp, rv;
+    load_source_f64(sg, w.s0 + tid, w.s1, rp, rv);
+    for (int t = 0; t < ntiles; ++t) {
+      const int buf = t & 1;
+      sp[buf][tid] = rp;
+      sv[buf][tid] = rv;
+      __syncthreads();
+      const int ts = w.s0 + t * TB;
+      if (t + 1 < ntiles) load_source_f64(sg, ts + TB + tid, w.s1, rp, rv);
+      const int skip = i - ts;
+#pragma unroll 2
+      for (int jj = 0; jj < TB; ++jj) {
+        const double4 p = sp[buf][jj];
+        const double4 s = sv[buf][jj];
+        const double dx = pi.x - p.x, dy = pi.y - p.y, dz = pi.z - p.z;
+        const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
+        const double sig2 = fma(0.5 * p.w, p.w, hi);
+        const double wr = rsqrt(r2 + sig2);
+        const double ri = rsqrt(r2);
+        const double ri2 = ri * ri;
+        const double w2 = wr * wr;
+        const double w4 = w2 * w2;
+        const double uu = sig2 * w2;
+        const double u2 = uu * uu;
+        const double u4 = u2 * u2;
+        double dp = u4 * uu * (w4 * wr);
+        const double zc = dp * sig2;
+        const double ph = fma(1.5, sig2, r2) * w4 * ri;
+        double qh = fma(-7.5, zc, ph) * sig2 * ri2;
+        const double fh = fma(2.5, zc, -qh) * ri2;
+        const double cx = fma(s.y, dz, -s.z * dy);
+        const double cy = fma(s.z, dx, -s.x * dz);
+        const double cz = fma(s.x, dy, -s.y * dx);
+        const double tt = fma(vi.z, cz, fma(vi.y, cy, vi.x * cx));
+        double ft = fh * tt;
+        const bool self = (jj == skip);
+        qh = self ? 0.0 : qh;
+        ft = self ? 0.0 : ft;
+        dp = self ? 0.0 : dp;
+        ux = fma(qh, cx, ux);
+        uy = fma(qh, cy, uy);
+        uz = fma(qh, cz, uz);
+        qx = fma(qh, s.x, qx);
+        qy = fma(qh, s.y, qy);
+        qz = fma(qh, s.z, qz);
+        gx = fma(ft, dx, gx);
+        gy = fma(ft, dy, gy);
+        gz = fma(ft, dz, gz);
+        if (DIFF) {
+          ex = fma(dp, s.x, ex);
+          ey = fma(dp, s.y, ey);
+          ez = fma(dp, s.z, ez);
+          ev = fma(dp, s.w, ev);
+        }
+      }
+    }
+
+    if (valid) {
+      const double A = kInv4Pi;
+      const double Qx = A * qx, Qy = A * qy, Qz = A * qz;
+      double dax = (vi.y * Qz - vi.z * Qy) + 3.0 * A * gx;
+      double day = (vi.z * Qx - vi.x * Qz) + 3.0 * A * gy;
+      double daz = (vi.x * Qy - vi.y * Qx) + 3.0 * A * gz;
+      if (DIFF) {
+        const double c = 15.0 * sg.nu * A;
+        dax += c * (vi.w * ex - ev * vi.x);
+        day += c * (vi.w * ey - ev * vi.y);
+        daz += c * (vi.w * ez - ev * vi.z);
+      }
+      const size_t n = (size_t)sg.n;
+      double *out = sg.partial + (size_t)w.chunk * 6 * n + i;
+      out[0] = A * ux;
+      out[n] = A * uy;
+      out[2 * n] = A * uz;
+      out[3 * n] = dax;
+      out[4 * n] = day;
+      out[5 * n] = daz;
+    }
+  }
+}
+
+using KernelFn = void (*)(const WorkItem *, int, const SegDesc *, int *);
+
+KernelFn select(const PairConfig &c, bool diffusion) {
+  if (c.p != 1) return nullptr;
+  if (c.tb == 128) return diffusion ? &pairs_f64_kernel<128, true> : &pairs_f64_kernel<128, false>;
+  if (c.tb == 256) return diffusion ? &pairs_f64_kernel<256, true> : &pairs_f64_kernel<256, false>;
+  return nullptr;
+}
+
+}  // namespace
+
+bool pairs_f64_supported(const PairConfig &c) { return select(c, true) != nullptr; }
+
+cudaError_t pairs_f64_occupancy(const PairConfig &c, bool diffusion, int *blocks_per_sm) {
+  KernelFn f = select(c, diffusion);
+  if (!f) return cudaErrorInvalidValue;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, c.tb, 0);
+}
+
+cudaError_t launch_pairs_f64(const PairConfig &c, bool diffusion, int grid, const WorkItem *items,
+                             int n_items, const SegDesc *segs, int *next_item, cudaStream_t s) {
+  KernelFn f = select(c, diffusion);
+  if (!f) return cudaErrorInvalidValue;
+  f<<<grid, c.tb, 0, s>>>(items, n_items, segs, next_item);
+  return cudaGetLastError();
+}
+
+}  // namespace pawan

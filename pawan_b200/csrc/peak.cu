@@ -1,0 +1,60 @@
+// Arithmetic-throughput probes used as roofline denominators: long chains of
+// independent FP32 FFMA (resp. FP64 DFMA), kPeakChains per thread, so the FMA
+// pipe, not latency, is the limit.  Each launched FMA counts 2 flops.
+#include "kernels.h"
+
+namespace pawan {
+namespace {
+
+__global__ void ffma_peak_kernel(int iters, float *sink) {
+  float a[kPeakChains];
+  const float m = 1.0f - 1e-7f * (float)(threadIdx.x & 7);
+  const float c = 1e-7f;
+#pragma unroll
+  for (int k = 0; k < kPeakChains; ++k) a[k] = (float)(threadIdx.x + k);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+#pragma unroll
+      for (int k = 0; k < kPeakChains; ++k) a[k] = fmaf(a[k], m, c);
+    }
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < kPeakChains; ++k) s += a[k];
+  if (s == 1234.5f) sink[blockIdx.x] = s;  // keeps the chains live
+}
+
+__global__ void dfma_peak_kernel(int iters, double *sink) {
+  double a[kPeakChains];
+  const double m = 1.0 - 1e-13 * (double)(threadIdx.x & 7);
+  const double c = 1e-13;
+#pragma unroll
+  for (int k = 0; k < kPeakChains; ++k) a[k] = (double)(threadIdx.x + k);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+#pragma unroll
+      for (int k = 0; k < kPeakChains; ++k) a[k] = fma(a[k], m, c);
+    }
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < kPeakChains; ++k) s += a[k];
+  if (s == 1234.5) sink[blockIdx.x] = s;
+}
+
+}  // namespace
+
+// FMAs launched: blocks * threads * iters * 16 * kPeakChains.
+cudaError_t launch_ffma_peak(int blocks, int threads, int iters, float *sink, cudaStream_t s) {
+  ffma_peak_kernel<<<blocks, threads, 0, s>>>(iters, sink);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dfma_peak(int blocks, int threads, int iters, double *sink, cudaStream_t s) {
+  dfma_peak_kernel<<<blocks, threads, 0, s>>>(iters, sink);
+  return cudaGetLastError();
+}
+
+}  // namespace pawan

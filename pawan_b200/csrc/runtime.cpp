@@ -1,0 +1,997 @@
+// Host runtime and C ABI of the pawan B200 library: contexts, systems (the
+// reference's __interaction with its wakes), execution plans over one or many
+// systems, RK4 driving, diagnostics, autotuning and throughput probes.
+#include "runtime.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+
+using namespace pawan;
+
+namespace pawan {
+
+int fail(pawan_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int cuda_fail(pawan_ctx *ctx, cudaError_t e, const char *where) {
+  std::string m = std::string(where) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  if (e == cudaErrorMemoryAllocation) return fail(ctx, PAWAN_ERR_NOMEM, m);
+  return fail(ctx, PAWAN_ERR_CUDA, m);
+}
+
+#define PAWAN_CUDA(ctx, expr)                                  \
+  do {                                                         \
+    cudaError_t e_ = (expr);                                   \
+    if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #expr); \
+  } while (0)
+
+#define PAWAN_TRY(expr)             \
+  do {                              \
+    int s_ = (expr);                \
+    if (s_ != PAWAN_OK) return s_;  \
+  } while (0)
+
+TileChoice default_tile(int precision) {
+  TileChoice t;
+  if (precision == PAWAN_PREC_F32) {
+    t.pc = PairConfig{128, 1, 4};
+  } else {
+    t.pc = PairConfig{128, 1, 1};
+  }
+  t.items_per_slot = 16;
+  return t;
+}
+
+std::vector<TileChoice> tile_candidates(int precision) {
+  std::vector<TileChoice> v;
+  if (precision == PAWAN_PREC_F32) {
+    for (int tb : {128, 256})
+      for (int p : {1, 2, 4})
+        for (int u : {2, 4}) {
+          TileChoice t;
+          t.pc = PairConfig{tb, p, u};
+          v.push_back(t);
+        }
+  } else {
+    for (int tb : {128, 256}) {
+      TileChoice t;
+      t.pc = PairConfig{tb, 1, 1};
+      v.push_back(t);
+    }
+  }
+  return v;
+}
+
+Plan::~Plan() {
+  if (graph_exec) cudaGraphExecDestroy(graph_exec);
+  if (graph) cudaGraphDestroy(graph);
+}
+
+bool Plan::stale() const {
+  for (size_t s = 0; s < systems.size(); ++s)
+    if (systems[s]->nu != nus[s]) return true;
+  return false;
+}
+
+static int occupancy(pawan_ctx *ctx, int precision, const PairConfig &pc, bool diffusion,
+                     int *bps) {
+  cudaError_t e;
+  if (precision == PAWAN_PREC_F32)
+    e = pairs_f32_occupancy(pc, diffusion, bps);
+  else if (precision == PAWAN_PREC_F64)
+    e = pairs_f64_occupancy(pc, diffusion, bps);
+  else
+    e = pairs_plain_occupancy(pc, bps);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "occupancy query");
+  if (*bps < 1) return fail(ctx, PAWAN_ERR_INVALID, "pair kernel does not fit on an SM");
+  return PAWAN_OK;
+}
+
+static bool tile_supported(int precision, const PairConfig &pc) {
+  if (precision == PAWAN_PREC_F32) return pairs_f32_supported(pc);
+  if (precision == PAWAN_PREC_F64) return pairs_f64_supported(pc);
+  return pairs_plain_supported(pc);
+}
+
+// Work decomposition.  Target tiles of tb/p particles; sources in chunks of
+// whole tb-tiles sized so that the launch holds about `items_per_slot` items
+// per resident block (or of `fixed_chunk_sources` when > 0, which makes a
+// system's arithmetic independent of the other systems in the plan).  Items are ordered largest first, so the dynamic
+// counter hands out the long ones early (longest-processing-time order).
+int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int precision,
+               const TileChoice &tile, std::unique_ptr<Plan> &out, int fixed_chunk_sources) {
+  if (systems.empty()) return fail(ctx, PAWAN_ERR_INVALID, "plan over no systems");
+  if (!tile_supported(precision, tile.pc))
+    return fail(ctx, PAWAN_ERR_INVALID, "unsupported pair tiling for this precision");
+  std::unique_ptr<Plan> p(new Plan());
+  p->systems = systems;
+  p->precision = precision;
+  p->tile = tile;
+  for (auto *s : systems) {
+    p->nus.push_back(s->nu);
+    if (s->nu != 0.0) p->diffusion = true;
+    p->interactions += (double)s->n * (double)s->n;
+  }
+  int bps = 0;
+  PAWAN_TRY(occupancy(ctx, precision, tile.pc, p->diffusion, &bps));
+  p->grid = ctx->sm_count * bps;
+  const int TB = tile.pc.tb;
+  const int TPB = targets_per_block(tile.pc);
+  const double slots = (double)p->grid;
+  const double target_pairs =
+      std::max(p->interactions / (slots * std::max(1, tile.items_per_slot)), (double)TPB * TB);
+
+  struct ItemCost {
+    WorkItem w;
+    double cost;
+  };
+  std::vector<ItemCost> items;
+  size_t partial_total = 0;
+  std::vector<size_t> partial_off(systems.size());
+  p->nchunks.resize(systems.size());
+  for (size_t s = 0; s < systems.size(); ++s) {
+    const int n = (int)systems[s]->n;
+    const int src_tiles = (n + TB - 1) / TB;
+    int tiles_per_chunk = fixed_chunk_sources > 0
+                              ? (fixed_chunk_sources + TB - 1) / TB
+                              : (int)std::ceil(target_pairs / ((double)TPB * TB));
+    tiles_per_chunk = std::max(1, std::min(tiles_per_chunk, src_tiles));
+    const int nch = (src_tiles + tiles_per_chunk - 1) / tiles_per_chunk;
+    p->nchunks[s] = nch;
+    partial_off[s] = partial_total;
+    partial_total += (size_t)nch * 6 * (size_t)n;
+    for (int c = 0; c < nch; ++c) {
+      const int s0 = c * tiles_per_chunk * TB;
+      const int s1 = std::min(n, (c + 1) * tiles_per_chunk * TB);
+      for (int t0 = 0; t0 < n; t0 += TPB) {
+        const int nt = std::min(TPB, n - t0);
+        items.push_back({WorkItem{(int)s, t0, c, s0, s1}, (double)nt * (double)(s1 - s0)});
+      }
+    }
+  }
+  std::stable_sort(items.begin(), items.end(),
+                   [](const ItemCost &a, const ItemCost &b) { return a.cost > b.cost; });
+  if (items.size() > (size_t)INT32_MAX) return fail(ctx, PAWAN_ERR_INVALID, "too many work items");
+  p->n_items = (int)items.size();
+
+  PAWAN_CUDA(ctx, p->partial.alloc(partial_total));
+  std::vector<WorkItem> wh(items.size());
+  for (size_t k = 0; k < items.size(); ++k) wh[k] = items[k].w;
+  std::vector<SegDesc> sh(systems.size());
+  std::vector<StageItem> sih;
+  p->stage_host.resize(systems.size());
+  for (size_t s = 0; s < systems.size(); ++s) {
+    pawan_system *y = systems[s];
+    SegDesc &d = sh[s];
+    d.pos32 = y->pos32.p;
+    d.vor32 = y->vor32.p;
+    d.pos64 = y->pos64.p;
+    d.vor64 = y->vor64.p;
+    d.partial = p->partial.p + partial_off[s];
+    d.n = (int)y->n;
+    d.nchunks = p->nchunks[s];
+    d.nu = y->nu;
+    StageDesc &g = p->stage_host[s];
+    g.partial = d.partial;
+    g.nchunks = d.nchunks;
+    g.n = d.n;
+    g.X = y->X.p;
+    g.Xs = y->Xs.p;
+    g.K1 = y->K1.p;
+    g.K2 = y->K2.p;
+    g.R = y->R.p;
+    g.rad = y->rad.p;
+    g.vol = y->vol.p;
+    g.pos32 = y->pos32.p;
+    g.vor32 = y->vor32.p;
+    g.pos64 = y->pos64.p;
+    g.vor64 = y->vor64.p;
+    g.dt = 0.0;
+    for (int l0 = 0; l0 < d.n; l0 += kStageThreads) sih.push_back(StageItem{(int)s, l0});
+  }
+  p->n_stage_blocks = (int)sih.size();
+  p->dts.assign(systems.size(), 0.0);
+  PAWAN_CUDA(ctx, p->items.alloc(wh.size()));
+  PAWAN_CUDA(ctx, p->segs.alloc(sh.size()));
+  PAWAN_CUDA(ctx, p->stage_items.alloc(sih.size()));
+  PAWAN_CUDA(ctx, p->stage_descs.alloc(sh.size()));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(p->items.p, wh.data(), wh.size() * sizeof(WorkItem),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(p->segs.p, sh.data(), sh.size() * sizeof(SegDesc),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(p->stage_items.p, sih.data(), sih.size() * sizeof(StageItem),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(p->stage_descs.p, p->stage_host.data(),
+                                  p->stage_host.size() * sizeof(StageDesc), cudaMemcpyHostToDevice,
+                                  ctx->stream));
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  out = std::move(p);
+  return PAWAN_OK;
+}
+
+// Puts each system's dt into the device stage table (only when it changed).
+int set_plan_dt(pawan_ctx *ctx, Plan &p, const double *dt, double dt0) {
+  bool changed = false;
+  for (size_t s = 0; s < p.systems.size(); ++s) {
+    const double v = dt ? dt[s] : dt0;
+    if (!(v > 0.0) || !std::isfinite(v)) return fail(ctx, PAWAN_ERR_INVALID, "dt must be positive");
+    if (p.dts[s] != v) {
+      p.dts[s] = v;
+      p.stage_host[s].dt = v;
+      changed = true;
+    }
+  }
+  if (changed) {
+    PAWAN_CUDA(ctx, cudaMemcpyAsync(p.stage_descs.p, p.stage_host.data(),
+                                    p.stage_host.size() * sizeof(StageDesc),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+  }
+  return PAWAN_OK;
+}
+
+static cudaEvent_t take_event(pawan_ctx *ctx) {
+  if (!ctx->event_pool.empty()) {
+    cudaEvent_t e = ctx->event_pool.back();
+    ctx->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  return e;
+}
+
+int launch_pairs(pawan_ctx *ctx, Plan &p, bool allow_events) {
+  PAWAN_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(int), ctx->stream));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ctx->profile && allow_events) {
+    e0 = take_event(ctx);
+    e1 = take_event(ctx);
+    if (!e0 || !e1) return fail(ctx, PAWAN_ERR_CUDA, "cannot create profiling events");
+    PAWAN_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
+  }
+  cudaError_t e;
+  if (p.precision == PAWAN_PREC_F32)
+    e = launch_pairs_f32(p.tile.pc, p.diffusion, p.grid, p.items.p, p.n_items, p.segs.p,
+                         ctx->d_counter, ctx->stream);
+  else if (p.precision == PAWAN_PREC_F64)
+    e = launch_pairs_f64(p.tile.pc, p.diffusion, p.grid, p.items.p, p.n_items, p.segs.p,
+                         ctx->d_counter, ctx->stream);
+  else
+    e = launch_pairs_plain(p.tile.pc, p.grid, p.items.p, p.n_items, p.segs.p, ctx->d_counter,
+                           ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "pair kernel launch");
+  ctx->launches++;
+  if (e0) {
+    PAWAN_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
+    ctx->pending.push_back({e0, e1});
+    ctx->pair_launches++;
+    ctx->pair_interactions += p.interactions;
+  }
+  return PAWAN_OK;
+}
+
+int launch_stage_mode(pawan_ctx *ctx, Plan &p, int mode) {
+  cudaError_t e = launch_stage(mode, PACK_F32 | PACK_F64, p.n_stage_blocks, p.stage_items.p,
+                               p.stage_descs.p, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "stage kernel launch");
+  ctx->launches++;
+  return PAWAN_OK;
+}
+
+static int rk4_one_step(pawan_ctx *ctx, Plan &p, bool allow_events) {
+  static const int modes[4] = {STAGE_K1, STAGE_K2, STAGE_K3, STAGE_FINAL};
+  for (int s = 0; s < 4; ++s) {
+    PAWAN_TRY(launch_pairs(ctx, p, allow_events));
+    PAWAN_TRY(launch_stage_mode(ctx, p, modes[s]));
+  }
+  return PAWAN_OK;
+}
+
+int rk4_steps(pawan_ctx *ctx, Plan &p, size_t nsteps, bool use_graph) {
+  if (!use_graph) {
+    for (size_t k = 0; k < nsteps; ++k) PAWAN_TRY(rk4_one_step(ctx, p, true));
+    return PAWAN_OK;
+  }
+  if (!p.graph_exec) {
+    PAWAN_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    const unsigned long long before = ctx->launches.load();
+    int st = rk4_one_step(ctx, p, false);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    ctx->launches = before;  // capture enqueues nothing; replays count below
+    if (st != PAWAN_OK) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "graph capture");
+    p.graph = g;
+    PAWAN_CUDA(ctx, cudaGraphInstantiate(&p.graph_exec, g, 0));
+  }
+  for (size_t k = 0; k < nsteps; ++k) {
+    PAWAN_CUDA(ctx, cudaGraphLaunch(p.graph_exec, ctx->stream));
+    ctx->launches += 8;
+  }
+  return PAWAN_OK;
+}
+
+int autotune_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int precision,
+                  TileChoice *best) {
+  cudaEvent_t e0, e1;
+  PAWAN_CUDA(ctx, cudaEventCreate(&e0));
+  PAWAN_CUDA(ctx, cudaEventCreate(&e1));
+  double best_ms = 1e300;
+  TileChoice best_t = default_tile(precision);
+  int status = PAWAN_OK;
+  auto time_tile = [&](const TileChoice &t, double *ms) -> int {
+    std::unique_ptr<Plan> p;
+    PAWAN_TRY(build_plan(ctx, systems, precision, t, p));
+    PAWAN_TRY(launch_pairs(ctx, *p, false));  // warm-up
+    PAWAN_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
+    const int reps = 2;
+    for (int r = 0; r < reps; ++r) PAWAN_TRY(launch_pairs(ctx, *p, false));
+    PAWAN_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
+    PAWAN_CUDA(ctx, cudaEventSynchronize(e1));
+    float f = 0.f;
+    PAWAN_CUDA(ctx, cudaEventElapsedTime(&f, e0, e1));
+    *ms = f / reps;
+    return PAWAN_OK;
+  };
+  // 1) tile shape at the default chunking, 2) chunking for the best shape.
+  for (const TileChoice &t : tile_candidates(precision)) {
+    double ms = 0;
+    status = time_tile(t, &ms);
+    if (status != PAWAN_OK) break;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best_t = t;
+    }
+  }
+  if (status == PAWAN_OK) {
+    for (int ips : {4, 8, 32}) {
+      TileChoice t = best_t;
+      t.items_per_slot = ips;
+      double ms = 0;
+      status = time_tile(t, &ms);
+      if (status != PAWAN_OK) break;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best_t = t;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (status == PAWAN_OK) *best = best_t;
+  return status;
+}
+
+int system_alloc(pawan_system *sys) {
+  pawan_ctx *ctx = sys->ctx;
+  const size_t n = sys->n;
+  PAWAN_CUDA(ctx, sys->X.alloc(6 * n));
+  PAWAN_CUDA(ctx, sys->Xs.alloc(6 * n));
+  PAWAN_CUDA(ctx, sys->K1.alloc(6 * n));
+  PAWAN_CUDA(ctx, sys->K2.alloc(6 * n));
+  PAWAN_CUDA(ctx, sys->R.alloc(6 * n));
+  PAWAN_CUDA(ctx, sys->rad.alloc(n));
+  PAWAN_CUDA(ctx, sys->vol.alloc(n));
+  PAWAN_CUDA(ctx, sys->wake_id.alloc(n));
+  PAWAN_CUDA(ctx, sys->pos32.alloc(n));
+  PAWAN_CUDA(ctx, sys->vor32.alloc(n));
+  PAWAN_CUDA(ctx, sys->pos64.alloc(n));
+  PAWAN_CUDA(ctx, sys->vor64.alloc(n));
+  PAWAN_CUDA(ctx, sys->diag_scratch.alloc(diag_scratch_doubles((int)n)));
+  PAWAN_CUDA(ctx, sys->diag_out.alloc(12));
+  std::vector<int> wid(n);
+  for (size_t w = 0; w < sys->counts.size(); ++w)
+    for (size_t i = 0; i < sys->counts[w]; ++i) wid[sys->offsets[w] + i] = (int)w;
+  PAWAN_CUDA(ctx, cudaMemcpy(sys->wake_id.p, wid.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  PAWAN_CUDA(ctx, cudaMemset(sys->X.p, 0, 6 * n * sizeof(double)));
+  return PAWAN_OK;
+}
+
+int system_ensure_plan(pawan_system *sys) {
+  if (!sys->has_particles)
+    return fail(sys->ctx, PAWAN_ERR_STATE, "particles not set (pawan_system_set_particles)");
+  if (sys->plan && !sys->plan->stale() && sys->plan->tile == sys->tile &&
+      sys->plan->precision == sys->precision)
+    return PAWAN_OK;
+  sys->plan.reset();
+  return build_plan(sys->ctx, {sys}, sys->precision, sys->tile, sys->plan);
+}
+
+// Reference layout (per wake [x | alpha]) -> device union layout [x | alpha].
+int state_to_device(pawan_system *sys, const double *state) {
+  pawan_ctx *ctx = sys->ctx;
+  const size_t N = sys->n;
+  for (size_t w = 0; w < sys->counts.size(); ++w) {
+    const size_t o = sys->offsets[w], c = sys->counts[w];
+    const double *src = state + 6 * o;
+    PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->X.p + 3 * o, src, 3 * c * sizeof(double),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+    PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->X.p + 3 * N + 3 * o, src + 3 * c, 3 * c * sizeof(double),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+  }
+  return PAWAN_OK;
+}
+
+// Device union layout -> reference layout; synchronous.
+int state_from_device(pawan_system *sys, const double *dev_union, double *state) {
+  pawan_ctx *ctx = sys->ctx;
+  const size_t N = sys->n;
+  for (size_t w = 0; w < sys->counts.size(); ++w) {
+    const size_t o = sys->offsets[w], c = sys->counts[w];
+    double *dst = state + 6 * o;
+    PAWAN_CUDA(ctx, cudaMemcpyAsync(dst, dev_union + 3 * o, 3 * c * sizeof(double),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+    PAWAN_CUDA(ctx, cudaMemcpyAsync(dst + 3 * c, dev_union + 3 * N + 3 * o, 3 * c * sizeof(double),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PAWAN_OK;
+}
+
+}  // namespace pawan
+
+size_t pawan_system::device_bytes() const {
+  return X.bytes() + Xs.bytes() + K1.bytes() + K2.bytes() + R.bytes() + rad.bytes() +
+         vol.bytes() + wake_id.bytes() + pos32.bytes() + vor32.bytes() + pos64.bytes() +
+         vor64.bytes() + diag_scratch.bytes() + diag_out.bytes() +
+         (plan ? plan->partial.bytes() : 0);
+}
+
+// =================================================================== C ABI
+
+#define CHECK_CTX(ctx) \
+  if (!(ctx)) return PAWAN_ERR_INVALID
+#define CHECK_SYS(sys) \
+  if (!(sys) || !(sys)->ctx) return PAWAN_ERR_INVALID
+
+static int pack_after_state(pawan_system *sys) {
+  PAWAN_TRY(system_ensure_plan(sys));
+  return launch_stage_mode(sys->ctx, *sys->plan, STAGE_PACK);
+}
+
+extern "C" {
+
+const char *pawan_status_name(int status) {
+  switch (status) {
+    case PAWAN_OK: return "ok";
+    case PAWAN_ERR_INVALID: return "invalid argument";
+    case PAWAN_ERR_CUDA: return "cuda error";
+    case PAWAN_ERR_NOMEM: return "out of memory";
+    case PAWAN_ERR_STATE: return "invalid state";
+    case PAWAN_ERR_BUDGET: return "exceeds budget";
+    case PAWAN_ERR_TIMEOUT: return "timeout";
+    case PAWAN_ERR_NOTFOUND: return "not found";
+    case PAWAN_ERR_REJECTED: return "rejected";
+    default: return "unknown status";
+  }
+}
+
+int pawan_ctx_create(int device, pawan_ctx **out) {
+  if (!out) return PAWAN_ERR_INVALID;
+  *out = nullptr;
+  std::unique_ptr<pawan_ctx> ctx(new pawan_ctx());
+  ctx->device = device;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || device < 0 || device >= count) return PAWAN_ERR_CUDA;
+  if (cudaSetDevice(device) != cudaSuccess) return PAWAN_ERR_CUDA;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return PAWAN_ERR_CUDA;
+  ctx->sm_count = prop.multiProcessorCount;
+  ctx->cc_major = prop.major;
+  ctx->cc_minor = prop.minor;
+  ctx->total_mem = prop.totalGlobalMem;
+  if (prop.major != 10) return PAWAN_ERR_CUDA;  // built for sm_100a only
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return PAWAN_ERR_CUDA;
+  if (cudaMalloc(&ctx->d_counter, sizeof(int)) != cudaSuccess) {
+    cudaStreamDestroy(ctx->stream);
+    return PAWAN_ERR_NOMEM;
+  }
+  *out = ctx.release();
+  return PAWAN_OK;
+}
+
+void pawan_ctx_destroy(pawan_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto &pr : ctx->pending) {
+    cudaEventDestroy(pr.first);
+    cudaEventDestroy(pr.second);
+  }
+  for (auto e : ctx->event_pool) cudaEventDestroy(e);
+  for (auto e : ctx->marks)
+    if (e) cudaEventDestroy(e);
+  if (ctx->flush_buf) cudaFree(ctx->flush_buf);
+  if (ctx->d_counter) cudaFree(ctx->d_counter);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char *pawan_ctx_last_error(const pawan_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int pawan_ctx_info(pawan_ctx *ctx, int *sm_count, int *cc_major, int *cc_minor, size_t *total_mem) {
+  CHECK_CTX(ctx);
+  if (sm_count) *sm_count = ctx->sm_count;
+  if (cc_major) *cc_major = ctx->cc_major;
+  if (cc_minor) *cc_minor = ctx->cc_minor;
+  if (total_mem) *total_mem = ctx->total_mem;
+  return PAWAN_OK;
+}
+
+int pawan_ctx_synchronize(pawan_ctx *ctx) {
+  CHECK_CTX(ctx);
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PAWAN_OK;
+}
+
+unsigned long long pawan_ctx_launch_count(const pawan_ctx *ctx) {
+  return ctx ? ctx->launches.load() : 0ull;
+}
+
+int pawan_ctx_profile(pawan_ctx *ctx, int enable) {
+  CHECK_CTX(ctx);
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (auto &pr : ctx->pending) {
+    ctx->event_pool.push_back(pr.first);
+    ctx->event_pool.push_back(pr.second);
+  }
+  ctx->pending.clear();
+  ctx->pair_ms = 0.0;
+  ctx->pair_launches = 0;
+  ctx->pair_interactions = 0.0;
+  ctx->profile = enable != 0;
+  return PAWAN_OK;
+}
+
+int pawan_ctx_profile_read(pawan_ctx *ctx, double *pair_ms, unsigned long long *pair_launches,
+                           double *pair_interactions) {
+  CHECK_CTX(ctx);
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (auto &pr : ctx->pending) {
+    float ms = 0.f;
+    PAWAN_CUDA(ctx, cudaEventElapsedTime(&ms, pr.first, pr.second));
+    ctx->pair_ms += ms;
+    ctx->event_pool.push_back(pr.first);
+    ctx->event_pool.push_back(pr.second);
+  }
+  ctx->pending.clear();
+  if (pair_ms) *pair_ms = ctx->pair_ms;
+  if (pair_launches) *pair_launches = ctx->pair_launches;
+  if (pair_interactions) *pair_interactions = ctx->pair_interactions;
+  return PAWAN_OK;
+}
+
+int pawan_ctx_mark(pawan_ctx *ctx, int slot) {
+  CHECK_CTX(ctx);
+  if (slot < 0 || slot >= 16) return fail(ctx, PAWAN_ERR_INVALID, "mark slot must be 0..15");
+  if (!ctx->marks[slot]) PAWAN_CUDA(ctx, cudaEventCreate(&ctx->marks[slot]));
+  PAWAN_CUDA(ctx, cudaEventRecord(ctx->marks[slot], ctx->stream));
+  return PAWAN_OK;
+}
+
+int pawan_ctx_elapsed(pawan_ctx *ctx, int slot0, int slot1, double *ms) {
+  CHECK_CTX(ctx);
+  if (!ms || slot0 < 0 || slot0 >= 16 || slot1 < 0 || slot1 >= 16 || !ctx->marks[slot0] ||
+      !ctx->marks[slot1])
+    return fail(ctx, PAWAN_ERR_INVALID, "unrecorded mark");
+  PAWAN_CUDA(ctx, cudaEventSynchronize(ctx->marks[slot1]));
+  float f = 0.f;
+  PAWAN_CUDA(ctx, cudaEventElapsedTime(&f, ctx->marks[slot0], ctx->marks[slot1]));
+  *ms = f;
+  return PAWAN_OK;
+}
+
+int pawan_ctx_flush_l2(pawan_ctx *ctx, size_t bytes) {
+  CHECK_CTX(ctx);
+  if (bytes > ctx->flush_bytes) {
+    if (ctx->flush_buf) cudaFree(ctx->flush_buf);
+    ctx->flush_buf = nullptr;
+    ctx->flush_bytes = 0;
+    PAWAN_CUDA(ctx, cudaMalloc(&ctx->flush_buf, bytes));
+    ctx->flush_bytes = bytes;
+  }
+  PAWAN_CUDA(ctx, cudaMemsetAsync(ctx->flush_buf, (int)(ctx->launches.load() & 0xff), bytes, ctx->stream));
+  return PAWAN_OK;
+}
+
+int pawan_host_alloc(pawan_ctx *ctx, size_t bytes, void **out) {
+  CHECK_CTX(ctx);
+  if (!out) return PAWAN_ERR_INVALID;
+  PAWAN_CUDA(ctx, cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocDefault));
+  return PAWAN_OK;
+}
+
+int pawan_host_free(pawan_ctx *ctx, void *ptr) {
+  CHECK_CTX(ctx);
+  PAWAN_CUDA(ctx, cudaFreeHost(ptr));
+  return PAWAN_OK;
+}
+
+int pawan_system_create(pawan_ctx *ctx, size_t n_wakes, const size_t *num_particles, double nu,
+                        int precision, pawan_system **out) {
+  CHECK_CTX(ctx);
+  if (!out || n_wakes == 0 || !num_particles)
+    return fail(ctx, PAWAN_ERR_INVALID, "system needs at least one wake");
+  if (precision < PAWAN_PREC_F32 || precision > PAWAN_PREC_F64_PLAIN)
+    return fail(ctx, PAWAN_ERR_INVALID, "unknown precision");
+  if (!std::isfinite(nu) || nu < 0.0) return fail(ctx, PAWAN_ERR_INVALID, "nu must be >= 0");
+  *out = nullptr;
+  std::unique_ptr<pawan_system> sys(new pawan_system());
+  sys->ctx = ctx;
+  size_t off = 0;
+  for (size_t w = 0; w < n_wakes; ++w) {
+    if (num_particles[w] == 0) return fail(ctx, PAWAN_ERR_INVALID, "empty wake");
+    sys->counts.push_back(num_particles[w]);
+    sys->offsets.push_back(off);
+    off += num_particles[w];
+  }
+  if (off < 2) return fail(ctx, PAWAN_ERR_INVALID, "a system needs at least two particles");
+  if (off > (size_t)(1 << 28)) return fail(ctx, PAWAN_ERR_INVALID, "too many particles");
+  sys->n = off;
+  sys->nu = nu;
+  sys->precision = precision;
+  sys->tile = default_tile(precision);
+  PAWAN_CUDA(ctx, cudaSetDevice(ctx->device));
+  PAWAN_TRY(system_alloc(sys.get()));
+  *out = sys.release();
+  return PAWAN_OK;
+}
+
+void pawan_system_destroy(pawan_system *sys) {
+  if (!sys) return;
+  if (sys->ctx) cudaStreamSynchronize(sys->ctx->stream);
+  delete sys;
+}
+
+size_t pawan_system_size(const pawan_system *sys) { return sys ? 6 * sys->n : 0; }
+size_t pawan_system_num_particles(const pawan_system *sys) { return sys ? sys->n : 0; }
+
+int pawan_system_set_particles(pawan_system *sys, const double *position, const double *vorticity,
+                               const double *radius, const double *volume) {
+  CHECK_SYS(sys);
+  pawan_ctx *ctx = sys->ctx;
+  if (!position || !vorticity || !radius || !volume)
+    return fail(ctx, PAWAN_ERR_INVALID, "null particle array");
+  const size_t N = sys->n;
+  for (size_t i = 0; i < N; ++i)
+    if (!(radius[i] > 0.0) || !std::isfinite(radius[i]))
+      return fail(ctx, PAWAN_ERR_INVALID, "smoothing radii must be positive");
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->X.p, position, 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->X.p + 3 * N, vorticity, 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->rad.p, radius, N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->vol.p, volume, N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  sys->has_particles = true;
+  PAWAN_TRY(pack_after_state(sys));
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PAWAN_OK;
+}
+
+int pawan_system_set_states(pawan_system *sys, const double *state, size_t size) {
+  CHECK_SYS(sys);
+  if (!state || size != 6 * sys->n)
+    return fail(sys->ctx, PAWAN_ERR_INVALID, "state size must be 6*N");
+  PAWAN_TRY(state_to_device(sys, state));
+  PAWAN_TRY(pack_after_state(sys));
+  PAWAN_CUDA(sys->ctx, cudaStreamSynchronize(sys->ctx->stream));
+  return PAWAN_OK;
+}
+
+int pawan_system_get_states(pawan_system *sys, double *state, size_t size) {
+  CHECK_SYS(sys);
+  if (!state || size != 6 * sys->n)
+    return fail(sys->ctx, PAWAN_ERR_INVALID, "state size must be 6*N");
+  return state_from_device(sys, sys->X.p, state);
+}
+
+int pawan_system_solve(pawan_system *sys) {
+  CHECK_SYS(sys);
+  PAWAN_TRY(system_ensure_plan(sys));
+  PAWAN_TRY(launch_pairs(sys->ctx, *sys->plan));
+  return launch_stage_mode(sys->ctx, *sys->plan, STAGE_RATES);
+}
+
+int pawan_system_get_rates(pawan_system *sys, double *rate, size_t size) {
+  CHECK_SYS(sys);
+  if (!rate || size != 6 * sys->n)
+    return fail(sys->ctx, PAWAN_ERR_INVALID, "rate size must be 6*N");
+  return state_from_device(sys, sys->R.p, rate);
+}
+
+int pawan_system_get_wake_rates(pawan_system *sys, size_t wake, double *velocity,
+                                double *retvorcity) {
+  CHECK_SYS(sys);
+  pawan_ctx *ctx = sys->ctx;
+  if (wake >= sys->counts.size() || !velocity || !retvorcity)
+    return fail(ctx, PAWAN_ERR_INVALID, "bad wake index or null output");
+  const size_t o = sys->offsets[wake], c = sys->counts[wake], N = sys->n;
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(velocity, sys->R.p + 3 * o, 3 * c * sizeof(double),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(retvorcity, sys->R.p + 3 * N + 3 * o, 3 * c * sizeof(double),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PAWAN_OK;
+}
+
+int pawan_system_rk4(pawan_system *sys, double dt, size_t nsteps) {
+  CHECK_SYS(sys);
+  PAWAN_TRY(system_ensure_plan(sys));
+  PAWAN_TRY(set_plan_dt(sys->ctx, *sys->plan, nullptr, dt));
+  return rk4_steps(sys->ctx, *sys->plan, nsteps, false);
+}
+
+int pawan_system_euler(pawan_system *sys, double dt, size_t nsteps) {
+  CHECK_SYS(sys);
+  PAWAN_TRY(system_ensure_plan(sys));
+  PAWAN_TRY(set_plan_dt(sys->ctx, *sys->plan, nullptr, dt));
+  for (size_t k = 0; k < nsteps; ++k) {
+    PAWAN_TRY(launch_pairs(sys->ctx, *sys->plan));
+    PAWAN_TRY(launch_stage_mode(sys->ctx, *sys->plan, STAGE_EULER));
+  }
+  return PAWAN_OK;
+}
+
+static int run_diagnostics(pawan_system *sys, bool quadratic, double *out12) {
+  pawan_ctx *ctx = sys->ctx;
+  if (!sys->has_particles) return fail(ctx, PAWAN_ERR_STATE, "particles not set");
+  cudaError_t e = launch_diagnostics((int)sys->n, sys->pos64.p, sys->vor64.p, sys->wake_id.p,
+                                     sys->diag_scratch.p, sys->diag_out.p, quadratic, ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "diagnostics launch");
+  ctx->launches += quadratic ? 4 : 2;
+  double h[12] = {0};
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(h, sys->diag_out.p, 12 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (!quadratic) h[9] = h[10] = h[11] = 0.0;
+  std::memcpy(out12, h, sizeof(h));
+  return PAWAN_OK;
+}
+
+int pawan_system_diagnose(pawan_system *sys, double *out, int quadratic) {
+  CHECK_SYS(sys);
+  if (!out) return fail(sys->ctx, PAWAN_ERR_INVALID, "null output");
+  double h[12];
+  PAWAN_TRY(run_diagnostics(sys, quadratic != 0, h));
+  std::memcpy(out, h, 11 * sizeof(double));
+  return PAWAN_OK;
+}
+
+int pawan_system_kinetic_energy(pawan_system *sys, double *ke) {
+  CHECK_SYS(sys);
+  if (!ke) return fail(sys->ctx, PAWAN_ERR_INVALID, "null output");
+  double h[12];
+  PAWAN_TRY(run_diagnostics(sys, true, h));
+  *ke = h[11];
+  return PAWAN_OK;
+}
+
+int pawan_system_set_nu(pawan_system *sys, double nu) {
+  CHECK_SYS(sys);
+  if (!std::isfinite(nu) || nu < 0.0) return fail(sys->ctx, PAWAN_ERR_INVALID, "nu must be >= 0");
+  sys->nu = nu;
+  return PAWAN_OK;
+}
+
+int pawan_system_set_precision(pawan_system *sys, int precision) {
+  CHECK_SYS(sys);
+  if (precision < PAWAN_PREC_F32 || precision > PAWAN_PREC_F64_PLAIN)
+    return fail(sys->ctx, PAWAN_ERR_INVALID, "unknown precision");
+  if (precision != sys->precision) {
+    sys->precision = precision;
+    if (!sys->fixed_tile || !tile_supported(precision, sys->tile.pc))
+      sys->tile = default_tile(precision);
+  }
+  return PAWAN_OK;
+}
+
+int pawan_system_write_frame(pawan_system *sys, const char *path, double t, int append) {
+  CHECK_SYS(sys);
+  pawan_ctx *ctx = sys->ctx;
+  if (!path) return fail(ctx, PAWAN_ERR_INVALID, "null path");
+  const size_t N = sys->n;
+  std::vector<double> x(6 * N), s(N);
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(x.data(), sys->X.p, 6 * N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(s.data(), sys->rad.p, N * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  FILE *f = std::fopen(path, append ? "ab" : "wb");
+  if (!f) return fail(ctx, PAWAN_ERR_INVALID, std::string("cannot open ") + path);
+  bool ok = std::fwrite(&t, sizeof(double), 1, f) == 1;
+  const size_t nw = sys->counts.size();
+  ok = ok && std::fwrite(&nw, sizeof(size_t), 1, f) == 1;
+  for (size_t w = 0; w < nw && ok; ++w) {
+    const size_t o = sys->offsets[w], c = sys->counts[w];
+    ok = ok && std::fwrite(&c, sizeof(size_t), 1, f) == 1;
+    ok = ok && std::fwrite(x.data() + 3 * o, sizeof(double), 3 * c, f) == 3 * c;
+    ok = ok && std::fwrite(x.data() + 3 * N + 3 * o, sizeof(double), 3 * c, f) == 3 * c;
+    ok = ok && std::fwrite(s.data() + o, sizeof(double), c, f) == c;
+  }
+  std::fclose(f);
+  if (!ok) return fail(ctx, PAWAN_ERR_INVALID, std::string("short write to ") + path);
+  return PAWAN_OK;
+}
+
+int pawan_system_set_config(pawan_system *sys, int threads, int threads_per_target, int unroll,
+                            int items_per_slot) {
+  CHECK_SYS(sys);
+  TileChoice t;
+  t.pc = PairConfig{threads, threads_per_target, unroll};
+  t.items_per_slot = items_per_slot;
+  if (items_per_slot < 1 || !tile_supported(sys->precision, t.pc))
+    return fail(sys->ctx, PAWAN_ERR_INVALID, "unsupported tiling for this precision");
+  sys->tile = t;
+  sys->fixed_tile = true;
+  return PAWAN_OK;
+}
+
+int pawan_system_get_config(pawan_system *sys, int *threads, int *threads_per_target, int *unroll,
+                            int *items_per_slot) {
+  CHECK_SYS(sys);
+  if (threads) *threads = sys->tile.pc.tb;
+  if (threads_per_target) *threads_per_target = sys->tile.pc.p;
+  if (unroll) *unroll = sys->tile.pc.unroll;
+  if (items_per_slot) *items_per_slot = sys->tile.items_per_slot;
+  return PAWAN_OK;
+}
+
+int pawan_system_autotune(pawan_system *sys) {
+  CHECK_SYS(sys);
+  if (!sys->has_particles) return fail(sys->ctx, PAWAN_ERR_STATE, "particles not set");
+  TileChoice best;
+  PAWAN_TRY(autotune_plan(sys->ctx, {sys}, sys->precision, &best));
+  sys->tile = best;
+  sys->fixed_tile = true;
+  sys->plan.reset();
+  const double n2 = (double)sys->n * (double)sys->n;
+  sys->ctx->tune_cache[std::make_tuple(sys->precision, sys->nu != 0.0 ? 1 : 0,
+                                       (int)std::log2(std::max(1.0, n2)), 0)] = best;
+  return system_ensure_plan(sys);
+}
+
+int pawan_system_device_state(pawan_system *sys, double **state) {
+  CHECK_SYS(sys);
+  if (!state) return PAWAN_ERR_INVALID;
+  *state = sys->X.p;
+  return PAWAN_OK;
+}
+
+// ------------------------------------------------------------------ batch
+
+struct pawan_batch {
+  pawan_ctx *ctx = nullptr;
+  std::vector<pawan_system *> systems;
+  int precision = PAWAN_PREC_F32;
+  TileChoice tile;
+  std::unique_ptr<Plan> plan;
+};
+
+static int batch_ensure_plan(pawan_batch *b) {
+  for (auto *s : b->systems)
+    if (!s->has_particles) return fail(b->ctx, PAWAN_ERR_STATE, "a batch system has no particles");
+  if (b->plan && !b->plan->stale() && b->plan->tile == b->tile) return PAWAN_OK;
+  b->plan.reset();
+  return build_plan(b->ctx, b->systems, b->precision, b->tile, b->plan);
+}
+
+int pawan_batch_create(pawan_ctx *ctx, size_t n, pawan_system *const *systems, pawan_batch **out) {
+  CHECK_CTX(ctx);
+  if (!out || n == 0 || !systems) return fail(ctx, PAWAN_ERR_INVALID, "empty batch");
+  std::unique_ptr<pawan_batch> b(new pawan_batch());
+  b->ctx = ctx;
+  b->precision = systems[0] ? systems[0]->precision : PAWAN_PREC_F32;
+  for (size_t i = 0; i < n; ++i) {
+    if (!systems[i] || systems[i]->ctx != ctx)
+      return fail(ctx, PAWAN_ERR_INVALID, "batch systems must share the context");
+    if (systems[i]->precision != b->precision)
+      return fail(ctx, PAWAN_ERR_INVALID, "batch systems must share one precision");
+    b->systems.push_back(systems[i]);
+  }
+  b->tile = default_tile(b->precision);
+  *out = b.release();
+  return PAWAN_OK;
+}
+
+void pawan_batch_destroy(pawan_batch *b) {
+  if (!b) return;
+  cudaStreamSynchronize(b->ctx->stream);
+  delete b;
+}
+
+int pawan_batch_rk4(pawan_batch *b, const double *dt, double dt0, size_t nsteps, int use_graph) {
+  if (!b) return PAWAN_ERR_INVALID;
+  PAWAN_TRY(batch_ensure_plan(b));
+  PAWAN_TRY(set_plan_dt(b->ctx, *b->plan, dt, dt0));
+  return rk4_steps(b->ctx, *b->plan, nsteps, use_graph != 0);
+}
+
+int pawan_batch_solve(pawan_batch *b) {
+  if (!b) return PAWAN_ERR_INVALID;
+  PAWAN_TRY(batch_ensure_plan(b));
+  PAWAN_TRY(launch_pairs(b->ctx, *b->plan));
+  return launch_stage_mode(b->ctx, *b->plan, STAGE_RATES);
+}
+
+int pawan_batch_set_config(pawan_batch *b, int threads, int threads_per_target, int unroll,
+                           int items_per_slot) {
+  if (!b) return PAWAN_ERR_INVALID;
+  TileChoice t;
+  t.pc = PairConfig{threads, threads_per_target, unroll};
+  t.items_per_slot = items_per_slot;
+  if (items_per_slot < 1 || !tile_supported(b->precision, t.pc))
+    return fail(b->ctx, PAWAN_ERR_INVALID, "unsupported tiling for this precision");
+  b->tile = t;
+  return PAWAN_OK;
+}
+
+int pawan_batch_autotune(pawan_batch *b) {
+  if (!b) return PAWAN_ERR_INVALID;
+  for (auto *s : b->systems)
+    if (!s->has_particles) return fail(b->ctx, PAWAN_ERR_STATE, "a batch system has no particles");
+  TileChoice best;
+  PAWAN_TRY(autotune_plan(b->ctx, b->systems, b->precision, &best));
+  b->tile = best;
+  b->plan.reset();
+  return batch_ensure_plan(b);
+}
+
+// ------------------------------------------------------------ throughput
+
+static int run_peak(pawan_ctx *ctx, double seconds, double *gflops, bool fp64) {
+  CHECK_CTX(ctx);
+  if (!gflops) return PAWAN_ERR_INVALID;
+  const int threads = 256;
+  const int blocks = ctx->sm_count * 8;
+  const int iters = fp64 ? 2048 : 4096;
+  DBuf<double> sink;
+  PAWAN_CUDA(ctx, sink.alloc((size_t)blocks));
+  cudaEvent_t e0, e1;
+  PAWAN_CUDA(ctx, cudaEventCreate(&e0));
+  PAWAN_CUDA(ctx, cudaEventCreate(&e1));
+  auto launch = [&]() -> cudaError_t {
+    ctx->launches++;
+    return fp64 ? launch_dfma_peak(blocks, threads, iters, sink.p, ctx->stream)
+                : launch_ffma_peak(blocks, threads, iters, reinterpret_cast<float *>(sink.p),
+                                   ctx->stream);
+  };
+  cudaError_t e = launch();  // warm-up
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  int launches = 0;
+  double ms_total = 0.0;
+  auto t0 = std::chrono::steady_clock::now();
+  while (e == cudaSuccess) {
+    e = cudaEventRecord(e0, ctx->stream);
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = launch();
+    if (e == cudaSuccess) e = cudaEventRecord(e1, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    ms_total += ms;
+    launches += 4;
+    if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() >= seconds)
+      break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "peak probe");
+  const double fmas = (double)launches * blocks * threads * (double)iters * 16.0 * kPeakChains;
+  *gflops = 2.0 * fmas / (ms_total * 1e-3) * 1e-9;
+  return PAWAN_OK;
+}
+
+int pawan_peak_fp32(pawan_ctx *ctx, double seconds, double *gflops) {
+  return run_peak(ctx, seconds, gflops, false);
+}
+
+int pawan_peak_fp64(pawan_ctx *ctx, double seconds, double *gflops) {
+  return run_peak(ctx, seconds, gflops, true);
+}
+
+}  // extern "C"

@@ -1,0 +1,152 @@
+// Internal host-side runtime of the pawan B200 library: context, systems,
+// execution plans.  Shared by the C-ABI (runtime.cpp) and the serving engine
+// (serve.cpp); not part of the public interface.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <map>
+#include <memory>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/pawan_b200.h"
+#include "kernels.h"
+
+namespace pawan {
+
+// A device allocation that frees itself.
+template <class T>
+struct DBuf {
+  T *p = nullptr;
+  size_t n = 0;
+  DBuf() = default;
+  DBuf(const DBuf &) = delete;
+  DBuf &operator=(const DBuf &) = delete;
+  ~DBuf() { reset(); }
+  cudaError_t alloc(size_t count) {
+    reset();
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&p), count * sizeof(T));
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    n = count;
+    return cudaSuccess;
+  }
+  void reset() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+// Tiling of the pair kernel plus how finely sources are chunked.
+struct TileChoice {
+  PairConfig pc{128, 1, 4};
+  int items_per_slot = 16;
+  bool operator==(const TileChoice &o) const {
+    return pc.tb == o.pc.tb && pc.p == o.pc.p && pc.unroll == o.pc.unroll &&
+           items_per_slot == o.items_per_slot;
+  }
+};
+
+TileChoice default_tile(int precision);
+std::vector<TileChoice> tile_candidates(int precision);
+
+struct Plan;
+
+}  // namespace pawan
+
+struct pawan_ctx {
+  int device = 0;
+  int sm_count = 0;
+  int cc_major = 0, cc_minor = 0;
+  size_t total_mem = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::atomic<unsigned long long> launches{0};
+  int *d_counter = nullptr;  // work-item counter of the persistent pair kernels
+  // profiling of pair launches
+  bool profile = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pending;
+  std::vector<cudaEvent_t> event_pool;
+  double pair_ms = 0.0;
+  unsigned long long pair_launches = 0;
+  double pair_interactions = 0.0;
+  cudaEvent_t marks[16] = {};
+  void *flush_buf = nullptr;
+  size_t flush_bytes = 0;
+  // autotune results: (precision, diffusion, log2 sum n^2, log2 segments) -> tile
+  std::map<std::tuple<int, int, int, int>, pawan::TileChoice> tune_cache;
+};
+
+struct pawan_system {
+  pawan_ctx *ctx = nullptr;
+  std::vector<size_t> counts;   // particles per wake
+  std::vector<size_t> offsets;  // first particle of each wake
+  size_t n = 0;
+  double nu = 0.0;
+  int precision = PAWAN_PREC_F32;
+  bool has_particles = false;
+  bool fixed_tile = false;
+  pawan::TileChoice tile;
+  pawan::DBuf<double> X, Xs, K1, K2, R, rad, vol, diag_scratch, diag_out;
+  pawan::DBuf<int> wake_id;
+  pawan::DBuf<float4> pos32, vor32;
+  pawan::DBuf<double4> pos64, vor64;
+  std::unique_ptr<pawan::Plan> plan;  // single-system plan for `tile`
+  double dt_uploaded = -1.0;
+  size_t device_bytes() const;
+};
+
+namespace pawan {
+
+// Everything one persistent pair launch plus its stage launch need for a set
+// of systems.  Owns the partial buffers and the device-side tables.
+struct Plan {
+  std::vector<pawan_system *> systems;
+  std::vector<double> nus;  // nu of each system when the plan was built
+  int precision = PAWAN_PREC_F32;
+  TileChoice tile;
+  bool diffusion = false;
+  int grid = 0;
+  int n_items = 0;
+  int n_stage_blocks = 0;
+  double interactions = 0.0;  // sum n^2
+  std::vector<int> nchunks;
+  DBuf<double> partial;
+  DBuf<WorkItem> items;
+  DBuf<SegDesc> segs;
+  DBuf<StageItem> stage_items;
+  DBuf<StageDesc> stage_descs;
+  std::vector<StageDesc> stage_host;
+  std::vector<double> dts;  // dt in the device stage table
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  ~Plan();
+  bool stale() const;
+};
+
+// Status helpers: record the message on the context and return the code.
+int fail(pawan_ctx *ctx, int code, const std::string &msg);
+int cuda_fail(pawan_ctx *ctx, cudaError_t e, const char *where);
+
+int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int precision,
+               const TileChoice &tile, std::unique_ptr<Plan> &out, int fixed_chunk_sources = 0);
+int set_plan_dt(pawan_ctx *ctx, Plan &p, const double *dt, double dt0);
+int launch_pairs(pawan_ctx *ctx, Plan &p, bool allow_events = true);
+int launch_stage_mode(pawan_ctx *ctx, Plan &p, int mode);
+int rk4_steps(pawan_ctx *ctx, Plan &p, size_t nsteps, bool use_graph);
+int autotune_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int precision,
+                  TileChoice *best);
+int system_alloc(pawan_system *sys);
+int system_ensure_plan(pawan_system *sys);
+int state_to_device(pawan_system *sys, const double *state);
+int state_from_device(pawan_system *sys, const double *dev_union, double *state);
+
+}  // namespace pawan

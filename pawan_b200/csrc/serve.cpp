@@ -1,0 +1,403 @@
+// Serving engine: a request loop with device-resident particle state and
+// continuous batching.
+//
+// Each request is a system (one ring, a ring pair, ...) with its own nu, dt
+// and step count.  The worker thread repeats: admit waiting requests in
+// arrival order while the device-memory budget, the active-request cap and the
+// per-iteration work cap (sum N^2) allow; advance every admitted request by
+// one RK4 step in one batched launch sequence (one persistent pair launch per
+// stage over all of them); retire the finished ones (state copied to the
+// host, device memory released).  Requests that arrive while others run join
+// at the next iteration, so their work overlaps on the device.
+//
+// Sources are chunked in fixed-size chunks per request, so a request's
+// arithmetic does not depend on which other requests share its launches: its
+// result is the same alone and in the mix, bit for bit.
+//
+// The engine owns its own context (stream, scheduler counter) on the device of
+// the context it was created from, so its worker never shares a stream with
+// the caller's thread.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+
+#include "runtime.h"
+
+using namespace pawan;
+
+namespace {
+
+constexpr int kServeChunkSources = 8192;
+
+double now_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+struct Request {
+  long long id = 0;
+  int state = PAWAN_REQ_QUEUED;
+  std::vector<size_t> counts;
+  std::vector<double> pos, vor, rad, vol;
+  double nu = 0.0, dt = 0.0;
+  size_t nsteps = 0, steps_done = 0;
+  size_t n = 0;
+  double bytes = 0.0;
+  double t_submit = 0.0, t_admit = -1.0, t_done = -1.0;
+  bool cancel = false;
+  pawan_system *sys = nullptr;
+  std::vector<double> result;
+};
+
+// Device bytes a request holds while active: the system's buffers plus its
+// partial chunks in a batched plan (fixed chunk size).
+double request_bytes(size_t n, int tb) {
+  const double per = 5 * 48.0 + 16.0 + 4.0 + 32.0 + 64.0;
+  const size_t chunk = ((kServeChunkSources + tb - 1) / tb) * (size_t)tb;
+  const size_t nch = (n + chunk - 1) / chunk;
+  return (double)n * per + 48.0 * (double)n * (double)nch + 4096.0;
+}
+
+}  // namespace
+
+struct pawan_server {
+  pawan_ctx *ctx = nullptr;  // owned, worker-thread only
+  pawan_serve_config cfg{};
+  std::thread worker;
+  std::mutex mu;
+  std::condition_variable cv_work, cv_done;
+  bool stop = false;
+  std::deque<long long> queue;
+  std::map<long long, std::unique_ptr<Request>> reqs;
+  std::vector<Request *> active;
+  long long next_id = 1;
+  std::chrono::steady_clock::time_point t0;
+  pawan_serve_stats stats{};
+  double bytes_in_use = 0.0;
+  std::string worker_error;
+  TileChoice tile;
+};
+
+namespace {
+
+void finish(pawan_server *srv, Request *r, int state) {
+  r->state = state;
+  r->t_done = now_since(srv->t0);
+}
+
+// One engine iteration on the admitted requests; called without the lock.
+int run_iteration(pawan_server *srv, std::vector<Request *> &act, std::unique_ptr<Plan> &plan,
+                  bool rebuild) {
+  pawan_ctx *ctx = srv->ctx;
+  if (rebuild || !plan) {
+    plan.reset();
+    std::vector<pawan_system *> sys;
+    for (Request *r : act) sys.push_back(r->sys);
+    int st = build_plan(ctx, sys, srv->cfg.precision, srv->tile, plan, kServeChunkSources);
+    if (st != PAWAN_OK) return st;
+  }
+  std::vector<double> dts;
+  for (Request *r : act) dts.push_back(r->dt);
+  int st = set_plan_dt(ctx, *plan, dts.data(), 0.0);
+  if (st != PAWAN_OK) return st;
+  st = rk4_steps(ctx, *plan, 1, false);
+  if (st != PAWAN_OK) return st;
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "serving iteration");
+  return PAWAN_OK;
+}
+
+void worker_main(pawan_server *srv) {
+  cudaSetDevice(srv->ctx->device);
+  std::unique_ptr<Plan> plan;
+  bool set_changed = true;
+  for (;;) {
+    std::vector<Request *> admit;
+    {
+      std::unique_lock<std::mutex> lk(srv->mu);
+      for (;;) {
+        // admission in arrival order (no overtaking), within all caps
+        if (srv->queue.empty()) break;
+        Request *r = srv->reqs[srv->queue.front()].get();
+        const size_t na = srv->active.size() + admit.size();
+        double n2 = (double)r->n * (double)r->n;
+        for (Request *a : srv->active) n2 += (double)a->n * (double)a->n;
+        for (Request *a : admit) n2 += (double)a->n * (double)a->n;
+        const bool empty = na == 0;
+        if (srv->bytes_in_use + r->bytes > srv->cfg.budget_bytes) break;
+        if (srv->cfg.max_active > 0 && (int)na >= srv->cfg.max_active) break;
+        if (srv->cfg.max_step_interactions > 0 && n2 > srv->cfg.max_step_interactions && !empty)
+          break;
+        srv->queue.pop_front();
+        srv->bytes_in_use += r->bytes;
+        r->state = PAWAN_REQ_ACTIVE;
+        r->t_admit = now_since(srv->t0);
+        admit.push_back(r);
+      }
+      if (srv->active.empty() && admit.empty()) {
+        if (srv->stop) break;
+        srv->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+        continue;
+      }
+      if (srv->stop && admit.empty() && srv->active.empty()) break;
+    }
+    // create device state of newly admitted requests (outside the lock)
+    for (Request *r : admit) {
+      int st = pawan_system_create(srv->ctx, r->counts.size(), r->counts.data(), r->nu,
+                                   srv->cfg.precision, &r->sys);
+      if (st == PAWAN_OK)
+        st = pawan_system_set_particles(r->sys, r->pos.data(), r->vor.data(), r->rad.data(),
+                                        r->vol.data());
+      std::lock_guard<std::mutex> lk(srv->mu);
+      if (st != PAWAN_OK) {
+        srv->worker_error = srv->ctx->err;
+        if (r->sys) pawan_system_destroy(r->sys);
+        r->sys = nullptr;
+        srv->bytes_in_use -= r->bytes;
+        finish(srv, r, PAWAN_REQ_REJECTED);
+        srv->stats.rejected++;
+        srv->cv_done.notify_all();
+        continue;
+      }
+      std::vector<double>().swap(r->pos);
+      std::vector<double>().swap(r->vor);
+      srv->active.push_back(r);
+      srv->stats.admitted++;
+      set_changed = true;
+    }
+    std::vector<Request *> act;
+    {
+      std::lock_guard<std::mutex> lk(srv->mu);
+      act = srv->active;
+    }
+    if (act.empty()) continue;
+    const auto it0 = std::chrono::steady_clock::now();
+    int st = run_iteration(srv, act, plan, set_changed);
+    set_changed = false;
+    const double busy = std::chrono::duration<double>(std::chrono::steady_clock::now() - it0).count();
+    // retire finished / cancelled requests
+    std::vector<Request *> done;
+    {
+      std::lock_guard<std::mutex> lk(srv->mu);
+      srv->stats.iterations++;
+      srv->stats.busy_seconds += busy;
+      if (st != PAWAN_OK) srv->worker_error = srv->ctx->err;
+      for (Request *r : act) {
+        if (st == PAWAN_OK) {
+          r->steps_done++;
+          srv->stats.interactions += 4.0 * (double)r->n * (double)r->n;
+        }
+        if (st != PAWAN_OK || r->cancel || r->steps_done >= r->nsteps) done.push_back(r);
+      }
+    }
+    for (Request *r : done) {
+      int state = PAWAN_REQ_DONE;
+      if (st != PAWAN_OK) {
+        state = PAWAN_REQ_REJECTED;
+      } else if (r->cancel) {
+        state = PAWAN_REQ_CANCELLED;
+      } else {
+        r->result.resize(6 * r->n);
+        if (pawan_system_get_states(r->sys, r->result.data(), r->result.size()) != PAWAN_OK)
+          state = PAWAN_REQ_REJECTED;
+      }
+      pawan_system_destroy(r->sys);
+      r->sys = nullptr;
+      std::lock_guard<std::mutex> lk(srv->mu);
+      srv->active.erase(std::find(srv->active.begin(), srv->active.end(), r));
+      srv->bytes_in_use -= r->bytes;
+      finish(srv, r, state);
+      if (state == PAWAN_REQ_DONE) srv->stats.completed++;
+      else if (state == PAWAN_REQ_REJECTED) srv->stats.rejected++;
+      set_changed = true;
+    }
+    if (!done.empty()) {
+      std::lock_guard<std::mutex> lk(srv->mu);
+      srv->cv_done.notify_all();
+    }
+  }
+  plan.reset();
+}
+
+}  // namespace
+
+extern "C" {
+
+int pawan_server_create(pawan_ctx *ctx, const pawan_serve_config *cfg, pawan_server **out) {
+  if (!ctx || !cfg || !out) return PAWAN_ERR_INVALID;
+  if (!(cfg->budget_bytes > 0) || cfg->precision < PAWAN_PREC_F32 ||
+      cfg->precision > PAWAN_PREC_F64_PLAIN)
+    return fail(ctx, PAWAN_ERR_INVALID, "bad serving configuration");
+  std::unique_ptr<pawan_server> srv(new pawan_server());
+  srv->cfg = *cfg;
+  srv->tile = default_tile(cfg->precision);
+  int st = pawan_ctx_create(ctx->device, &srv->ctx);
+  if (st != PAWAN_OK) return fail(ctx, st, "cannot create the serving context");
+  srv->t0 = std::chrono::steady_clock::now();
+  pawan_server *raw = srv.get();
+  try {
+    srv->worker = std::thread(worker_main, raw);
+  } catch (...) {
+    pawan_ctx_destroy(srv->ctx);
+    return fail(ctx, PAWAN_ERR_NOMEM, "cannot start the serving thread");
+  }
+  *out = srv.release();
+  return PAWAN_OK;
+}
+
+void pawan_server_destroy(pawan_server *srv) {
+  if (!srv) return;
+  {
+    std::lock_guard<std::mutex> lk(srv->mu);
+    srv->stop = true;
+    // queued requests never start; active ones are cancelled at the next iteration
+    for (long long id : srv->queue) finish(srv, srv->reqs[id].get(), PAWAN_REQ_CANCELLED);
+    srv->queue.clear();
+    for (Request *r : srv->active) r->cancel = true;
+  }
+  srv->cv_work.notify_all();
+  if (srv->worker.joinable()) srv->worker.join();
+  for (auto &kv : srv->reqs)
+    if (kv.second->sys) pawan_system_destroy(kv.second->sys);
+  pawan_ctx_destroy(srv->ctx);
+  delete srv;
+}
+
+int pawan_server_submit(pawan_server *srv, size_t n_wakes, const size_t *num_particles,
+                        const double *position, const double *vorticity, const double *radius,
+                        const double *volume, double nu, double dt, size_t nsteps,
+                        long long *id) {
+  if (!srv || !id || n_wakes == 0 || !num_particles || !position || !vorticity || !radius ||
+      !volume || nsteps == 0 || !(dt > 0) || !(nu >= 0))
+    return PAWAN_ERR_INVALID;
+  std::unique_ptr<Request> r(new Request());
+  size_t n = 0;
+  for (size_t w = 0; w < n_wakes; ++w) {
+    if (num_particles[w] == 0) return PAWAN_ERR_INVALID;
+    r->counts.push_back(num_particles[w]);
+    n += num_particles[w];
+  }
+  if (n < 2) return PAWAN_ERR_INVALID;
+  r->n = n;
+  r->nu = nu;
+  r->dt = dt;
+  r->nsteps = nsteps;
+  r->bytes = request_bytes(n, srv->tile.pc.tb);
+  std::lock_guard<std::mutex> lk(srv->mu);
+  r->id = srv->next_id++;
+  r->t_submit = now_since(srv->t0);
+  *id = r->id;
+  srv->stats.submitted++;
+  if (srv->stop) {
+    finish(srv, r.get(), PAWAN_REQ_REJECTED);
+    srv->stats.rejected++;
+    srv->reqs[r->id] = std::move(r);
+    return PAWAN_ERR_REJECTED;
+  }
+  if (r->bytes > srv->cfg.budget_bytes) {
+    finish(srv, r.get(), PAWAN_REQ_REJECTED);
+    srv->stats.rejected++;
+    srv->reqs[r->id] = std::move(r);
+    return PAWAN_ERR_BUDGET;
+  }
+  if (srv->cfg.max_queue > 0 && (int)srv->queue.size() >= srv->cfg.max_queue) {
+    finish(srv, r.get(), PAWAN_REQ_REJECTED);
+    srv->stats.rejected++;
+    srv->reqs[r->id] = std::move(r);
+    return PAWAN_ERR_REJECTED;
+  }
+  r->pos.assign(position, position + 3 * n);
+  r->vor.assign(vorticity, vorticity + 3 * n);
+  r->rad.assign(radius, radius + n);
+  r->vol.assign(volume, volume + n);
+  srv->queue.push_back(r->id);
+  srv->reqs[r->id] = std::move(r);
+  srv->cv_work.notify_all();
+  return PAWAN_OK;
+}
+
+int pawan_server_poll(pawan_server *srv, long long id, int *state) {
+  if (!srv || !state) return PAWAN_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(srv->mu);
+  auto it = srv->reqs.find(id);
+  if (it == srv->reqs.end()) return PAWAN_ERR_NOTFOUND;
+  *state = it->second->state;
+  return PAWAN_OK;
+}
+
+int pawan_server_wait(pawan_server *srv, long long id, double timeout_s) {
+  if (!srv) return PAWAN_ERR_INVALID;
+  std::unique_lock<std::mutex> lk(srv->mu);
+  auto deadline = std::chrono::steady_clock::now() +
+                  std::chrono::duration_cast<std::chrono::steady_clock::duration>(
+                      std::chrono::duration<double>(std::max(0.0, timeout_s)));
+  for (;;) {
+    auto it = srv->reqs.find(id);
+    if (it == srv->reqs.end()) return PAWAN_ERR_NOTFOUND;
+    const int s = it->second->state;
+    if (s == PAWAN_REQ_DONE || s == PAWAN_REQ_REJECTED || s == PAWAN_REQ_CANCELLED)
+      return PAWAN_OK;
+    if (srv->cv_done.wait_until(lk, deadline) == std::cv_status::timeout) {
+      auto it2 = srv->reqs.find(id);
+      if (it2 != srv->reqs.end()) {
+        const int s2 = it2->second->state;
+        if (s2 == PAWAN_REQ_DONE || s2 == PAWAN_REQ_REJECTED || s2 == PAWAN_REQ_CANCELLED)
+          return PAWAN_OK;
+      }
+      return PAWAN_ERR_TIMEOUT;
+    }
+  }
+}
+
+int pawan_server_fetch(pawan_server *srv, long long id, double *state, size_t size,
+                       double *t_submit, double *t_admit, double *t_done) {
+  if (!srv) return PAWAN_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(srv->mu);
+  auto it = srv->reqs.find(id);
+  if (it == srv->reqs.end()) return PAWAN_ERR_NOTFOUND;
+  Request *r = it->second.get();
+  if (r->state == PAWAN_REQ_QUEUED || r->state == PAWAN_REQ_ACTIVE) return PAWAN_ERR_STATE;
+  if (t_submit) *t_submit = r->t_submit;
+  if (t_admit) *t_admit = r->t_admit;
+  if (t_done) *t_done = r->t_done;
+  const int s = r->state;
+  if (s == PAWAN_REQ_DONE) {
+    if (!state || size != r->result.size()) return PAWAN_ERR_INVALID;
+    std::memcpy(state, r->result.data(), size * sizeof(double));
+  }
+  srv->reqs.erase(it);
+  return s == PAWAN_REQ_DONE ? PAWAN_OK : (s == PAWAN_REQ_CANCELLED ? PAWAN_ERR_STATE : PAWAN_ERR_REJECTED);
+}
+
+int pawan_server_cancel(pawan_server *srv, long long id) {
+  if (!srv) return PAWAN_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(srv->mu);
+  auto it = srv->reqs.find(id);
+  if (it == srv->reqs.end()) return PAWAN_ERR_NOTFOUND;
+  Request *r = it->second.get();
+  if (r->state == PAWAN_REQ_QUEUED) {
+    srv->queue.erase(std::find(srv->queue.begin(), srv->queue.end(), id));
+    finish(srv, r, PAWAN_REQ_CANCELLED);
+    srv->cv_done.notify_all();
+  } else if (r->state == PAWAN_REQ_ACTIVE) {
+    r->cancel = true;
+  }
+  return PAWAN_OK;
+}
+
+int pawan_server_stats(pawan_server *srv, pawan_serve_stats *out) {
+  if (!srv || !out) return PAWAN_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(srv->mu);
+  *out = srv->stats;
+  out->queued = srv->queue.size();
+  out->active = srv->active.size();
+  out->bytes_in_use = srv->bytes_in_use;
+  return PAWAN_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,144 @@
+// Per-particle stage kernel: reduces the pair kernel's partial chunks in fixed
+// chunk order into the rates (u | dalpha), applies the RK4 stage update in
+// FP64 with the reference's operation order, and packs the new state into the
+// FP32 / FP64 tile arrays the next pair launch reads.  One thread per particle,
+// HBM-bound.
+//
+// Reference: __rk4::step (src/integration/rk4.cpp:12-76):
+//   x1 = k1*(0.5 dt) + x        (:29-31)      STAGE_K1
+//   x2 = k2*(0.5 dt) + x        (:39-41)      STAGE_K2
+//   x3 = k3*dt + x              (:49-51)      STAGE_K3 (also forms k2 + k3, :61)
+//   x += (k1 + k4)*(dt/6) + (k2 + k3)*(dt/3)   (:58-66)   STAGE_FINAL
+// and __integration::step (src/integration/integration.cpp:37-45): x += r*dt.
+// Products and sums use __dmul_rn/__dadd_rn so no multiply-add is contracted,
+// keeping the update bit-identical to the reference's for equal rates.
+#include "device.cuh"
+#include "kernels.h"
+
+namespace pawan {
+namespace {
+
+__device__ __forceinline__ void pack(const StageDesc &d, int l, const double x[6], int flags) {
+  const double s = d.rad[l];
+  const double v = d.vol[l];
+  if (flags & PACK_F32) {
+    d.pos32[l] = make_float4((float)x[0], (float)x[1], (float)x[2], (float)(0.5 * s * s));
+    d.vor32[l] = make_float4((float)x[3], (float)x[4], (float)x[5], (float)v);
+  }
+  if (flags & PACK_F64) {
+    d.pos64[l] = make_double4(x[0], x[1], x[2], s);
+    d.vor64[l] = make_double4(x[3], x[4], x[5], v);
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kStageThreads)
+    stage_kernel(const StageItem *__restrict__ items, const StageDesc *__restrict__ descs,
+                 int pack_flags) {
+  const StageItem it = items[blockIdx.x];
+  const StageDesc d = descs[it.seg];
+  const int l = it.l0 + threadIdx.x;
+  if (l >= d.n) return;
+  const size_t n = (size_t)d.n;
+  size_t idx[6];
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    idx[k] = 3 * (size_t)l + k;
+    idx[3 + k] = 3 * n + 3 * (size_t)l + k;
+  }
+
+  double r[6];
+  if (MODE != STAGE_PACK) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) r[k] = d.partial[(size_t)k * n + l];
+    for (int c = 1; c < d.nchunks; ++c) {
+      const double *p = d.partial + (size_t)c * 6 * n + l;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) r[k] = __dadd_rn(r[k], p[(size_t)k * n]);
+    }
+  }
+
+  // Per-segment step size; the coefficients are formed as the reference forms
+  // them (0.5*dt, dt/6., dt/3.), and device division is correctly rounded.
+  const double dt = d.dt;
+  const double half = 0.5 * dt;
+  const double full = dt;
+  const double sixth = dt / 6.;
+  const double third = dt / 3.;
+
+  double x[6];
+  if (MODE == STAGE_RATES) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) d.R[idx[k]] = r[k];
+    return;
+  } else if (MODE == STAGE_K1 || MODE == STAGE_K2) {
+    double *K = (MODE == STAGE_K1) ? d.K1 : d.K2;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      K[idx[k]] = r[k];
+      x[k] = __dadd_rn(__dmul_rn(r[k], half), d.X[idx[k]]);
+      d.Xs[idx[k]] = x[k];
+    }
+  } else if (MODE == STAGE_K3) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      d.K2[idx[k]] = __dadd_rn(d.K2[idx[k]], r[k]);
+      x[k] = __dadd_rn(__dmul_rn(r[k], full), d.X[idx[k]]);
+      d.Xs[idx[k]] = x[k];
+    }
+  } else if (MODE == STAGE_FINAL) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      const double a = __dmul_rn(__dadd_rn(d.K1[idx[k]], r[k]), sixth);
+      const double b = __dmul_rn(d.K2[idx[k]], third);
+      x[k] = __dadd_rn(d.X[idx[k]], __dadd_rn(a, b));
+      d.X[idx[k]] = x[k];
+    }
+  } else if (MODE == STAGE_EULER) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+      x[k] = __dadd_rn(d.X[idx[k]], __dmul_rn(r[k], full));
+      d.X[idx[k]] = x[k];
+    }
+  } else {  // STAGE_PACK
+#pragma unroll
+    for (int k = 0; k < 6; ++k) x[k] = d.X[idx[k]];
+  }
+  pack(d, l, x, pack_flags);
+}
+
+}  // namespace
+
+cudaError_t launch_stage(int mode, int pack_flags, int n_blocks, const StageItem *items,
+                         const StageDesc *descs, cudaStream_t s) {
+  if (n_blocks <= 0) return cudaSuccess;
+  dim3 grid(n_blocks), block(kStageThreads);
+  switch (mode) {
+    case STAGE_RATES:
+      stage_kernel<STAGE_RATES><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      break;
+    case STAGE_K1:
+      stage_kernel<STAGE_K1><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      break;
+    case STAGE_K2:
+      stage_kernel<STAGE_K2><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      break;
+    case STAGE_K3:
+      stage_kernel<STAGE_K3><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      break;
+    case STAGE_FINAL:
+      stage_kernel<STAGE_FINAL><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      break;
+    case STAGE_EULER:
+      stage_kernel<STAGE_EULER><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      break;
+    case STAGE_PACK:
+      stage_kernel<STAGE_PACK><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace pawan

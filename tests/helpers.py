@@ -1,0 +1,46 @@
+"""Shared test helpers: error metrics with the stated tolerances, golden fixtures."""
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+# Stated tolerances (relative to the FP64 reference values):
+#   FP32 pair math with FP64 accumulation: RMS relative error <= 1e-5,
+#     max-abs error / max-abs reference <= 1e-4;
+#   FP64 kernels: RMS relative error <= 1e-12, max-norm error <= 1e-11.
+TOL_F32_RMS = 1e-5
+TOL_F32_MAX = 1e-4
+TOL_F64_RMS = 1e-12
+TOL_F64_MAX = 1e-11
+
+
+def rms_rel(a, b) -> float:
+    a, b = np.asarray(a, dtype=np.float64).ravel(), np.asarray(b, dtype=np.float64).ravel()
+    den = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a - b))
+
+
+def max_rel(a, b) -> float:
+    a, b = np.asarray(a, dtype=np.float64).ravel(), np.asarray(b, dtype=np.float64).ravel()
+    den = np.abs(b).max()
+    return float(np.abs(a - b).max() / den) if den > 0 else float(np.abs(a - b).max())
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+def split_rates(counts, rates):
+    """Reference rate vector -> (u, dalpha) union arrays."""
+    us, das, o = [], [], 0
+    for c in counts:
+        blk = rates[6 * o: 6 * (o + c)]
+        us.append(blk[:3 * c].reshape(c, 3))
+        das.append(blk[3 * c:].reshape(c, 3))
+        o += c
+    return np.concatenate(us), np.concatenate(das)
+
+
+def tol(precision):
+    return (TOL_F32_RMS, TOL_F32_MAX) if precision == "f32" else (TOL_F64_RMS, TOL_F64_MAX)

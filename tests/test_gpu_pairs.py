@@ -1,0 +1,172 @@
+"""Parity of the CUDA all-pairs interaction with the reference, through the C ABI.
+
+Tolerances (tests/helpers.py): FP32 pair math with FP64 accumulation -- RMS
+relative error <= 1e-5 and max error <= 1e-4 of the max reference value, for
+velocity and vorticity rate separately; FP64 kernels -- RMS <= 1e-12, max <= 1e-11.
+"""
+import numpy as np
+import pytest
+
+import oracle
+import pawan_b200
+from pawan_b200 import System
+from pawan_b200 import geometry as g
+from helpers import load, max_rel, rms_rel, split_rates, tol
+
+pytestmark = pytest.mark.gpu
+
+PRECS = ["f32", "f64", "f64_plain"]
+
+
+def check(prec, u, da, u_ref, da_ref):
+    t_rms, t_max = tol(prec)
+    assert rms_rel(u, u_ref) <= t_rms, ("u rms", rms_rel(u, u_ref))
+    assert rms_rel(da, da_ref) <= t_rms, ("da rms", rms_rel(da, da_ref))
+    assert max_rel(u, u_ref) <= t_max, ("u max", max_rel(u, u_ref))
+    assert max_rel(da, da_ref) <= t_max, ("da max", max_rel(da, da_ref))
+
+
+@pytest.mark.parametrize("prec", PRECS)
+@pytest.mark.parametrize("name", ["ring64_solve", "pair64_solve", "helix3_solve"])
+def test_solve_matches_reference_golden(ctx, name, prec):
+    d = load(name)
+    counts = [int(c) for c in d["counts"]]
+    s = System(ctx, counts, float(d["nu"]), prec)
+    s.set_particles(d["pos"], d["vor"], d["rad"], d["vol"])
+    s.solve()
+    rates = s.get_rates()
+    u, da = split_rates(counts, rates)
+    u_ref, da_ref = split_rates(counts, d["rates"])
+    check(prec, u, da, u_ref, da_ref)
+    # per-wake accessor agrees with the rate vector
+    uu, dd = s.union_rates()
+    assert np.array_equal(uu, u) and np.array_equal(dd, da)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("prec", PRECS)
+def test_solve_matches_reference_fresh(ctx, prec):
+    sc = g.ring_pair(n_stations=40, seed=202, nu=7e-4)  # N = 640, two wakes
+    pos, vor, rad, vol = sc.union()
+    ref = oracle.RefSystem(sc.counts, pos, vor, rad, vol, sc.nu)
+    ref.solve()
+    s = System.from_scenario(ctx, sc, prec)
+    s.solve()
+    check(prec, *s.union_rates(), *ref.union_rates())
+    assert np.array_equal(s.get_rates(), s.get_rates())
+
+
+@pytest.mark.parametrize("n", [2, 3, 31, 127, 128, 129, 255, 257, 1000, 4099])
+def test_ragged_sizes_against_restatement(ctx, n):
+    rng = np.random.default_rng(n)
+    pos = rng.uniform(-1, 1, (n, 3))
+    vor = rng.normal(0, 0.01, (n, 3))
+    rad = rng.uniform(0.05, 0.2, n)
+    vol = rng.uniform(1e-4, 2e-4, n)
+    u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, 1e-3)
+    for prec in PRECS:
+        s = System(ctx, [n], 1e-3, prec)
+        s.set_particles(pos, vor, rad, vol)
+        s.solve()
+        check(prec, *s.union_rates(), u_ref, da_ref)
+
+
+def test_many_wakes_union(ctx):
+    """Five wakes of uneven size: all pairs over the union, like interact()."""
+    rng = np.random.default_rng(5)
+    counts = [17, 200, 1, 64, 333]
+    n = sum(counts)
+    pos = rng.uniform(-1, 1, (n, 3))
+    vor = rng.normal(0, 0.01, (n, 3))
+    rad = rng.uniform(0.05, 0.2, n)
+    vol = rng.uniform(1e-4, 2e-4, n)
+    u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, 2e-3)
+    s = System(ctx, counts, 2e-3, "f32")
+    s.set_particles(pos, vor, rad, vol)
+    s.solve()
+    check("f32", *s.union_rates(), u_ref, da_ref)
+
+
+@pytest.mark.parametrize("tb", [128, 256])
+@pytest.mark.parametrize("p", [1, 2, 4])
+@pytest.mark.parametrize("unroll", [2, 4])
+def test_every_f32_tiling(ctx, tb, p, unroll):
+    sc = g.ring_pair(n_stations=70, seed=33, nu=1e-3)  # N = 1120: ragged tiles
+    pos, vor, rad, vol = sc.union()
+    u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, sc.nu)
+    s = System.from_scenario(ctx, sc, "f32")
+    for ips in (1, 16, 64):
+        s.set_config(tb, p, unroll, ips)
+        s.solve()
+        check("f32", *s.union_rates(), u_ref, da_ref)
+
+
+def test_nu_zero_matches_and_set_nu(ctx):
+    sc = g.single_ring(n_stations=50, seed=8, nu=0.0)
+    pos, vor, rad, vol = sc.union()
+    s = System.from_scenario(ctx, sc, "f32")
+    s.solve()
+    check("f32", *s.union_rates(), *oracle.pairs(pos, vor, rad, vol, 0.0))
+    s.set_nu(5e-3)
+    s.solve()
+    check("f32", *s.union_rates(), *oracle.pairs(pos, vor, rad, vol, 5e-3))
+
+
+def test_deterministic_bits(ctx):
+    sc = g.ring_pair(n_stations=300, seed=9, nu=1e-4)
+    s = System.from_scenario(ctx, sc, "f32")
+    s.solve()
+    a = s.get_rates()
+    for _ in range(3):
+        s.solve()
+        assert np.array_equal(s.get_rates(), a)
+
+
+def test_total_vorticity_rate_conserved(ctx):
+    """Pair terms are antisymmetric, so sum dalpha = 0 up to rounding."""
+    sc = g.ring_pair(n_stations=256, seed=10, nu=1e-3)
+    s = System.from_scenario(ctx, sc, "f32")
+    s.solve()
+    _, da = s.union_rates()
+    assert np.abs(da.sum(axis=0)).max() < 1e-5 * np.abs(da).sum()
+
+
+def test_state_roundtrip_exact(ctx):
+    sc = g.helical_wake(n_stations=12, seed=4, filaments=3, turns=1.0)
+    s = System.from_scenario(ctx, sc, "f32")
+    st = sc.state()
+    assert np.array_equal(s.get_states(), st)
+    st2 = st + 1e-3
+    s.set_states(st2)
+    assert np.array_equal(s.get_states(), st2)
+
+
+def test_invalid_arguments_raise(ctx):
+    with pytest.raises(pawan_b200.PawanError):
+        System(ctx, [], 0.0)
+    with pytest.raises(pawan_b200.PawanError):
+        System(ctx, [1], 0.0)  # a single particle interacts with nothing
+    with pytest.raises(pawan_b200.PawanError):
+        System(ctx, [10], -1.0)
+    s = System(ctx, [10], 0.0)
+    with pytest.raises(pawan_b200.PawanError):
+        s.solve()  # no particles yet
+    with pytest.raises(pawan_b200.PawanError):
+        s.set_config(96, 1, 2, 16)
+
+
+@pytest.mark.parametrize("name", ["ring_pair", "helical_wake"])
+def test_full_size_sampled_targets(ctx, name):
+    """N = 131,072 (ring pair) and 262,144 (helical wake) in FP32: sampled
+    targets against the FP64 restatement summing over all N sources."""
+    sc = g.ring_pair(steps=1) if name == "ring_pair" else g.helical_wake(steps=1)
+    pos, vor, rad, vol = sc.union()
+    s = System.from_scenario(ctx, sc, "f32")
+    s.solve()
+    u, da = s.union_rates()
+    rng = np.random.default_rng(0)
+    t = np.sort(rng.choice(sc.n, 512, replace=False))
+    u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, sc.nu, targets=t)
+    check("f32", u[t], da[t], u_ref, da_ref)
+    _, da_all = u, da
+    assert np.abs(da_all.sum(axis=0)).max() < 1e-5 * np.abs(da_all).sum()

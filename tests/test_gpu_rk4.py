@@ -1,0 +1,139 @@
+"""Parity of the device-resident integrators and diagnostics with the reference,
+through the C ABI.
+
+RK4 / Euler: compared on the state increments (final - initial), which is where
+the integrator's arithmetic shows; FP64 paths to 1e-11 RMS, FP32 pair math to
+the FP32 tolerance.  Diagnostics in FP64 against the reference's diagnose().
+Drift: over the full single-ring run (N = 2,048, 200 steps, dt = 0.01) the
+conserved quantities of the FP32 trajectory stay within stated bounds of the
+FP64 trajectory's.
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle
+from pawan_b200 import System, union_to_state
+from pawan_b200 import geometry as g
+from helpers import TOL_F32_RMS, load, rms_rel
+
+pytestmark = pytest.mark.gpu
+
+
+def make(ctx, d, prec):
+    s = System(ctx, [int(c) for c in d["counts"]], float(d["nu"]), prec)
+    s.set_particles(d["pos"], d["vor"], d["rad"], d["vol"])
+    return s
+
+
+@pytest.mark.parametrize("prec,tol", [("f64_plain", 1e-11), ("f64", 1e-11), ("f32", TOL_F32_RMS)])
+@pytest.mark.parametrize("name", ["ring64_rk4", "pair64_rk4"])
+def test_rk4_matches_reference_golden(ctx, name, prec, tol):
+    d = load(name)
+    s = make(ctx, d, prec)
+    s.rk4(float(d["dt"]), int(d["nsteps"]))
+    out = s.get_states()
+    assert rms_rel(out - d["state"], d["final_state"] - d["state"]) <= tol
+
+
+@pytest.mark.parametrize("prec,tol", [("f64_plain", 1e-11), ("f32", TOL_F32_RMS)])
+def test_euler_matches_reference_golden(ctx, prec, tol):
+    d = load("pair64_euler")
+    s = make(ctx, d, prec)
+    s.euler(float(d["dt"]), int(d["nsteps"]))
+    out = s.get_states()
+    assert rms_rel(out - d["state"], d["final_state"] - d["state"]) <= tol
+
+
+def test_rk4_update_is_bitwise_reference_order(ctx):
+    """With the plain FP64 kernel, one step from identical inputs differs from
+    the reference only through the pair sums' rounding; the update itself uses
+    the reference's operation order, so two runs agree bit for bit."""
+    d = load("ring64_rk4")
+    a, b = make(ctx, d, "f64_plain"), make(ctx, d, "f64_plain")
+    a.rk4(0.01, 2)
+    b.rk4(0.01, 1)
+    b.rk4(0.01, 1)
+    assert np.array_equal(a.get_states(), b.get_states())
+
+
+def test_diagnostics_match_reference_golden(ctx):
+    d = load("pair64_diag")
+    s = make(ctx, d, "f32")
+    r = s.diagnose()
+    scale = np.abs(d["vor"]).sum()
+    assert np.abs(r["total_vorticity"] - d["total_vorticity"]).max() < 1e-14 * scale
+    r2a = (np.linalg.norm(d["pos"], axis=1) ** 2 * np.linalg.norm(d["vor"], axis=1)).sum()
+    assert np.abs(r["linear_impulse"] - d["linear_impulse"]).max() < 1e-14 * r2a
+    assert np.abs(r["angular_impulse"] - d["angular_impulse"]).max() < 1e-14 * r2a
+    assert abs(r["enstrophy"] / d["enstrophy"] - 1) < 1e-12
+    assert abs(r["helicity"] - d["helicity"]) < 1e-10 * abs(d["enstrophy"])
+    assert abs(s.kinetic_energy() / d["kinetic_energy"] - 1) < 1e-12
+    lin = s.diagnose(quadratic=False)
+    assert lin["enstrophy"] == 0.0 and np.array_equal(lin["linear_impulse"], r["linear_impulse"])
+
+
+def test_diagnostics_match_restatement_larger(ctx):
+    sc = g.helical_wake(n_stations=64, seed=12, filaments=4, turns=2.0)  # N = 2048
+    pos, vor, rad, vol = sc.union()
+    s = System.from_scenario(ctx, sc, "f32")
+    r = s.diagnose()
+    assert abs(r["enstrophy"] / oracle.enstrophy(pos, vor, rad) - 1) < 1e-12
+    assert abs(r["helicity"] - oracle.helicity(pos, vor, rad)) < 1e-10 * abs(r["enstrophy"])
+    ke = oracle.kinetic_energy(sc.wake_ids(), pos, vor, rad)
+    assert abs(s.kinetic_energy() / ke - 1) < 1e-12
+
+
+def test_rk4_short_trajectory_against_restatement(ctx):
+    """Single ring, N = 2,048, 10 steps of dt = 0.01 (nu = 0)."""
+    sc = g.single_ring()
+    pos, vor, rad, vol = sc.union()
+    p, v = oracle.rk4_step(pos, vor, rad, vol, sc.nu, sc.dt, 10)
+    ref = union_to_state(sc.counts, p, v)
+    st0 = sc.state()
+    for prec, tol in (("f64_plain", 1e-11), ("f32", TOL_F32_RMS)):
+        s = System.from_scenario(ctx, sc, prec)
+        s.rk4(sc.dt, 10)
+        assert rms_rel(s.get_states() - st0, ref - st0) <= tol, prec
+
+
+def test_full_single_ring_drift(ctx):
+    """The full plain-FP64 workload (N = 2,048, 200 RK4 steps): the FP32 run's
+    conserved quantities track the FP64 run's.  Bounds: total vorticity and
+    linear impulse within 1e-6 relative of the FP64 values, enstrophy within
+    1e-5 relative; the FP32 state increment within 1e-4 RMS of FP64's."""
+    sc = g.single_ring()
+    runs = {}
+    for prec in ("f64_plain", "f32"):
+        s = System.from_scenario(ctx, sc, prec)
+        s.rk4(sc.dt, sc.steps)
+        runs[prec] = (s.get_states(), s.diagnose())
+    st0 = sc.state()
+    (x64, d64), (x32, d32) = runs["f64_plain"], runs["f32"]
+    assert rms_rel(x32 - st0, x64 - st0) < 1e-4
+    scale_o = np.abs(sc.union()[1]).sum()
+    assert np.abs(d32["total_vorticity"] - d64["total_vorticity"]).max() < 1e-6 * scale_o
+    assert rms_rel(d32["linear_impulse"], d64["linear_impulse"]) < 1e-6
+    assert abs(d32["enstrophy"] / d64["enstrophy"] - 1) < 1e-5
+
+
+def test_wake_frames_match_reference_format(ctx):
+    d = load("ring16_integrate")
+    s = make(ctx, d, "f64_plain")
+    T, n = float(d["T"]), int(d["nsteps"])
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "run.wake")
+        s.write_frame(path, 0.0, append=False)
+        for i in range(1, n + 1):
+            s.rk4(T / n, 1)
+            s.write_frame(path, i * (T / n), append=True)
+        raw = open(path, "rb").read()
+    ref = d["wake_bytes"].tobytes()
+    assert len(raw) == len(ref)
+    a = np.frombuffer(raw, dtype=np.float64)
+    b = np.frombuffer(ref, dtype=np.float64)
+    # headers (t, counts) identical; particle data within FP64 rounding
+    assert np.array_equal(a[:3], b[:3])
+    assert np.allclose(a, b, rtol=1e-12, atol=1e-15)

@@ -1,0 +1,113 @@
+"""The continuous-batching serving loop: results alone vs in the mix,
+admission by memory budget, queue limits, cancellation."""
+import time
+
+import numpy as np
+import pytest
+
+from pawan_b200 import Server, System
+from pawan_b200 import geometry as g
+from helpers import TOL_F32_RMS, rms_rel
+
+pytestmark = pytest.mark.gpu
+
+
+def requests(k=5, seed=7):
+    reqs = g.serving_requests(rate=1000.0, duration=1.0, seed=seed, n_lo=64, n_hi=1200,
+                              steps_lo=2, steps_hi=6)
+    return [r.scenario for r in reqs[:k]]
+
+
+def run_alone(ctx, sc):
+    srv = Server(ctx, budget_bytes=1 << 30)
+    st, rid = srv.submit_scenario(sc)
+    assert st == 0
+    assert srv.wait(rid, 60)
+    out, *_ = srv.fetch(rid)
+    srv.close()
+    return out
+
+
+def test_alone_and_in_the_mix_are_identical(ctx):
+    scs = requests()
+    srv = Server(ctx, budget_bytes=1 << 30)
+    ids = []
+    for k, sc in enumerate(scs):
+        st, rid = srv.submit_scenario(sc)
+        assert st == 0
+        ids.append(rid)
+        time.sleep(0.002 * k)  # staggered arrivals join running iterations
+    for rid in ids:
+        assert srv.wait(rid, 120)
+    mixed = [srv.fetch(rid) for rid in ids]
+    stats = srv.stats()
+    srv.close()
+    assert stats["completed"] == len(scs) and stats["rejected"] == 0
+    for sc, (out, ts, ta, td) in zip(scs, mixed):
+        assert out is not None and ts <= ta <= td
+        alone = run_alone(ctx, sc)
+        assert np.array_equal(out, alone)
+        solo = System.from_scenario(ctx, sc, "f32")
+        solo.rk4(sc.dt, sc.steps)
+        st0 = sc.state()
+        assert rms_rel(out - st0, solo.get_states() - st0) < 1e-12
+
+
+def test_budget_rejects_oversized_request(ctx):
+    srv = Server(ctx, budget_bytes=1e5)
+    sc = g.single_ring(n_stations=64, seed=1)
+    st, rid = srv.submit_scenario(sc, nsteps=1)
+    assert st == 5  # exceeds budget
+    assert srv.poll(rid) == "rejected"
+    srv.close()
+
+
+def test_budget_serialises_admission(ctx):
+    """A budget that fits one request at a time: all finish, never two active."""
+    scs = [g.single_ring(n_stations=128, seed=s, steps=3) for s in (1, 2, 3)]
+    probe = Server(ctx, budget_bytes=1 << 30)
+    rid = probe.submit_scenario(scs[0], nsteps=400)[1]
+    while probe.poll(rid) == "queued":
+        time.sleep(0.001)
+    one = probe.stats()["bytes_in_use"]
+    probe.cancel(rid)
+    probe.close()
+    assert one > 0
+    srv = Server(ctx, budget_bytes=one * 1.5)
+    ids = [srv.submit_scenario(sc)[1] for sc in scs]
+    peak_active = 0
+    deadline = time.time() + 120
+    while time.time() < deadline:
+        s = srv.stats()
+        peak_active = max(peak_active, s["active"])
+        if s["completed"] == len(scs):
+            break
+        time.sleep(0.001)
+    assert srv.stats()["completed"] == len(scs)
+    assert peak_active <= 1
+    for rid in ids:
+        out, *_ = srv.fetch(rid)
+        assert out is not None
+    srv.close()
+
+
+def test_queue_limit_and_cancel(ctx):
+    sc = g.single_ring(n_stations=64, seed=2)
+    srv = Server(ctx, budget_bytes=1 << 30, max_active=1, max_queue=2)
+    ids, sts = [], []
+    for _ in range(6):
+        st, rid = srv.submit_scenario(sc, nsteps=200)
+        ids.append(rid)
+        sts.append(st)
+    assert sts.count(8) >= 1  # queue full -> rejected
+    queued = [rid for rid, st in zip(ids, sts) if st == 0 and srv.poll(rid) == "queued"]
+    if queued:
+        srv.cancel(queued[-1])
+        assert srv.poll(queued[-1]) == "cancelled"
+    for rid, st in zip(ids, sts):
+        if st == 0:
+            srv.cancel(rid)
+    for rid, st in zip(ids, sts):
+        if st == 0:
+            assert srv.wait(rid, 60)
+    srv.close()
