@@ -161,6 +161,11 @@ class Context:
                                  "(needs a B200 / sm_100 device)")
         self._h = h
         self.device = device
+        import weakref
+        self._children = weakref.WeakSet()
+
+    def _adopt(self, child):
+        self._children.add(child)
 
     @property
     def handle(self):
@@ -172,7 +177,10 @@ class Context:
             raise PawanError(st, msg.decode() if msg else "")
 
     def close(self):
+        """Destroys the context, after the systems, batches and servers made on it."""
         if getattr(self, "_h", None):
+            for child in list(getattr(self, "_children", ())):
+                child.close()
             self._lib.pawan_ctx_destroy(self._h)
             self._h = None
 
@@ -256,6 +264,7 @@ class System:
         ctx.check(self._lib.pawan_system_create(ctx.handle, len(self.counts), cnt.ctypes.data_as(_szp),
                                                 float(nu), PREC[precision], ctypes.byref(h)))
         self._h = h
+        ctx._adopt(self)
         self.n = sum(self.counts)
         self.size = 6 * self.n
         self.nu = nu
@@ -369,6 +378,7 @@ class Batch:
         h = _vp()
         ctx.check(self._lib.pawan_batch_create(ctx.handle, len(self.systems), arr, ctypes.byref(h)))
         self._h = h
+        ctx._adopt(self)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -412,6 +422,7 @@ class Server:
         ctx.check(self._lib.pawan_server_create(ctx.handle, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
         self._sizes = {}
+        ctx._adopt(self)
 
     def close(self):
         if getattr(self, "_h", None):

@@ -7,10 +7,15 @@
 //                      this per wake, wake.cpp:87-120; the host API converts)
 //   rad    double[N]   smoothing radius s          (wake.h:39)
 //   vol    double[N]   particle volume v           (wake.h:40)
-//   pos32  float4[N]   (x, y, z, s^2/2)   packed FP32 source/target tile data
-//   vor32  float4[N]   (ax, ay, az, v)    32 bytes per particle in total
-//   pos64  double4[N]  (x, y, z, s)       packed FP64 data (FP64 kernels)
-//   vor64  double4[N]  (ax, ay, az, v)
+//   pos32  float4[N]   (x-c, y-c, z-c, s^2/2)  packed FP32 tile data: position
+//                      relative to the system's origin c, rounded to FP32 (hi)
+//   poslo  float4[N]   (x-c - hi, ..., 0)  what the FP32 rounding dropped (lo)
+//   vor32  float4[N]   (ax, ay, az, v)    strength (hi) and volume
+//   vorlo  float4[N]   (ax - hi, ..., 0)  strength (lo)
+//                      -> 64 bytes per particle; hi + lo carries ~48 bits
+//   pos64  double4[N]  (x, y, z, s)       packed FP64 data (FP64 kernels,
+//   vor64  double4[N]  (ax, ay, az, v)     diagnostics)
+//   boxes  float4[2 per source tile]  bounding box of each tile's hi positions
 //   partial double[C][6][N]  per source-chunk sums (u, dalpha) of the pair
 //                      kernel, reduced in fixed chunk order by the stage kernel
 #pragma once
@@ -24,12 +29,16 @@ namespace pawan {
 struct SegDesc {
   const float4 *pos32;
   const float4 *vor32;
+  const float4 *poslo;
+  const float4 *vorlo;
   const double4 *pos64;
   const double4 *vor64;
-  double *partial;  // [nchunks][6][n]
+  const float4 *boxes;  // [2 * ceil(n / tile)] (lo, hi) per source tile
+  double *partial;      // [nchunks][6][n]
   int n;
   int nchunks;
   double nu;
+  float near2;          // squared box distance below which a tile pair is "near"
 };
 
 // One unit of pair work: targets [t0, t0 + targets_per_block) of segment `seg`
@@ -63,8 +72,13 @@ struct StageDesc {
   const double *vol;
   float4 *pos32;
   float4 *vor32;
+  float4 *poslo;
+  float4 *vorlo;
   double4 *pos64;
   double4 *vor64;
+  float4 *boxes;     // per box_tile particles: (lo, hi)
+  int box_tile;      // 128 or 256 (divides kStageThreads)
+  double ox, oy, oz; // origin the FP32 positions are relative to
   double dt;
 };
 
@@ -78,13 +92,12 @@ enum StageMode : int {
   STAGE_PACK = 6,    // pack x only
 };
 
-enum PackFlags : int { PACK_F32 = 1, PACK_F64 = 2 };
-
 // 1/(4 pi) and friends.
 constexpr double kInv4Pi = 0.07957747154594766788;
 constexpr double kInvPi = 0.31830988618379067154;
 
-// Block sizes.
+// Block sizes.  Source tiles (and so bounding boxes) are 128 or 256
+// particles; stage blocks cover whole tiles.
 constexpr int kStageThreads = 256;
 
 }  // namespace pawan

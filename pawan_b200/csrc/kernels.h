@@ -38,8 +38,8 @@ cudaError_t launch_pairs_plain(const PairConfig &c, int grid, const WorkItem *it
                                const SegDesc *segs, int *next_item, cudaStream_t s);
 
 // Per-particle stage kernel (reduce partials, RK4 stage update, pack).
-cudaError_t launch_stage(int mode, int pack_flags, int n_blocks, const StageItem *items,
-                         const StageDesc *descs, cudaStream_t s);
+cudaError_t launch_stage(int mode, int n_blocks, const StageItem *items, const StageDesc *descs,
+                         cudaStream_t s);
 
 // Diagnostics of one system.  `scratch` holds at least diag_scratch_doubles(n)
 // doubles; out[0..10] = total vorticity (3), linear impulse (3), angular

@@ -1,5 +1,7 @@
-// All-pairs interaction in FP64 with the algebra of the FP32 kernel
-// (pair_f32.cu): two rsqrt per pair, no pow, no division.  This is the
+// All-pairs interaction in FP64 with the kernel algebra of the FP32 kernel
+// (pair_f32.cu): two rsqrt per pair, no pow, no division; the stretching and
+// diffusion vectors per pair as the reference forms them (alpha_i x alpha_j,
+// v_i alpha_j - v_j alpha_i).  This is the
 // "tuned FP64" variant, reported beside the FP32 kernel and the plain FP64
 // comparator (pair_plain.cu).  Same work items, partial layout and gather form.
 //
@@ -51,7 +53,7 @@ __global__ void __launch_bounds__(TB)
     }
     const double hi = 0.5 * pi.w * pi.w;
     double ux = 0, uy = 0, uz = 0, qx = 0, qy = 0, qz = 0, gx = 0, gy = 0, gz = 0;
-    double ex = 0, ey = 0, ez = 0, ev = 0;
+    double ex = 0, ey = 0, ez = 0;
 
     const int ntiles = (w.s1 - w.s0 + TB - 1) / TB;
     double4 rp, rv;
@@ -87,7 +89,10 @@ __global__ void __launch_bounds__(TB)
         const double cx = fma(s.y, dz, -s.z * dy);
         const double cy = fma(s.z, dx, -s.x * dz);
         const double cz = fma(s.x, dy, -s.y * dx);
-        const double tt = fma(vi.z, cz, fma(vi.y, cy, vi.x * cx));
+        const double wx = fma(vi.y, s.z, -vi.z * s.y);
+        const double wy = fma(vi.z, s.x, -vi.x * s.z);
+        const double wz = fma(vi.x, s.y, -vi.y * s.x);
+        const double tt = fma(dz, wz, fma(dy, wy, dx * wx));
         double ft = fh * tt;
         const bool self = (jj == skip);
         qh = self ? 0.0 : qh;
@@ -96,32 +101,30 @@ __global__ void __launch_bounds__(TB)
         ux = fma(qh, cx, ux);
         uy = fma(qh, cy, uy);
         uz = fma(qh, cz, uz);
-        qx = fma(qh, s.x, qx);
-        qy = fma(qh, s.y, qy);
-        qz = fma(qh, s.z, qz);
+        qx = fma(qh, wx, qx);
+        qy = fma(qh, wy, qy);
+        qz = fma(qh, wz, qz);
         gx = fma(ft, dx, gx);
         gy = fma(ft, dy, gy);
         gz = fma(ft, dz, gz);
         if (DIFF) {
-          ex = fma(dp, s.x, ex);
-          ey = fma(dp, s.y, ey);
-          ez = fma(dp, s.z, ez);
-          ev = fma(dp, s.w, ev);
+          ex = fma(dp, fma(vi.w, s.x, -s.w * vi.x), ex);
+          ey = fma(dp, fma(vi.w, s.y, -s.w * vi.y), ey);
+          ez = fma(dp, fma(vi.w, s.z, -s.w * vi.z), ez);
         }
       }
     }
 
     if (valid) {
       const double A = kInv4Pi;
-      const double Qx = A * qx, Qy = A * qy, Qz = A * qz;
-      double dax = (vi.y * Qz - vi.z * Qy) + 3.0 * A * gx;
-      double day = (vi.z * Qx - vi.x * Qz) + 3.0 * A * gy;
-      double daz = (vi.x * Qy - vi.y * Qx) + 3.0 * A * gz;
+      double dax = A * qx + 3.0 * A * gx;
+      double day = A * qy + 3.0 * A * gy;
+      double daz = A * qz + 3.0 * A * gz;
       if (DIFF) {
         const double c = 15.0 * sg.nu * A;
-        dax += c * (vi.w * ex - ev * vi.x);
-        day += c * (vi.w * ey - ev * vi.y);
-        daz += c * (vi.w * ez - ev * vi.z);
+        dax += c * ex;
+        day += c * ey;
+        daz += c * ez;
       }
       const size_t n = (size_t)sg.n;
       double *out = sg.partial + (size_t)w.chunk * 6 * n + i;

@@ -75,7 +75,8 @@ Plan::~Plan() {
 
 bool Plan::stale() const {
   for (size_t s = 0; s < systems.size(); ++s)
-    if (systems[s]->nu != nus[s]) return true;
+    if (systems[s]->nu != nus[s] || systems[s]->geometry_version != geometry_versions[s])
+      return true;
   return false;
 }
 
@@ -115,6 +116,8 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
   p->tile = tile;
   for (auto *s : systems) {
     p->nus.push_back(s->nu);
+    p->geometry_versions.push_back(s->geometry_version);
+    p->box_versions.push_back(~0ull);
     if (s->nu != 0.0) p->diffusion = true;
     p->interactions += (double)s->n * (double)s->n;
   }
@@ -132,8 +135,8 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     double cost;
   };
   std::vector<ItemCost> items;
-  size_t partial_total = 0;
-  std::vector<size_t> partial_off(systems.size());
+  size_t partial_total = 0, box_total = 0;
+  std::vector<size_t> partial_off(systems.size()), box_off(systems.size());
   p->nchunks.resize(systems.size());
   for (size_t s = 0; s < systems.size(); ++s) {
     const int n = (int)systems[s]->n;
@@ -146,6 +149,8 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     p->nchunks[s] = nch;
     partial_off[s] = partial_total;
     partial_total += (size_t)nch * 6 * (size_t)n;
+    box_off[s] = box_total;
+    box_total += 2 * (size_t)src_tiles;
     for (int c = 0; c < nch; ++c) {
       const int s0 = c * tiles_per_chunk * TB;
       const int s1 = std::min(n, (c + 1) * tiles_per_chunk * TB);
@@ -161,6 +166,7 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
   p->n_items = (int)items.size();
 
   PAWAN_CUDA(ctx, p->partial.alloc(partial_total));
+  PAWAN_CUDA(ctx, p->boxes.alloc(box_total));
   std::vector<WorkItem> wh(items.size());
   for (size_t k = 0; k < items.size(); ++k) wh[k] = items[k].w;
   std::vector<SegDesc> sh(systems.size());
@@ -171,12 +177,16 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     SegDesc &d = sh[s];
     d.pos32 = y->pos32.p;
     d.vor32 = y->vor32.p;
+    d.poslo = y->poslo.p;
+    d.vorlo = y->vorlo.p;
     d.pos64 = y->pos64.p;
     d.vor64 = y->vor64.p;
+    d.boxes = p->boxes.p + box_off[s];
     d.partial = p->partial.p + partial_off[s];
     d.n = (int)y->n;
     d.nchunks = p->nchunks[s];
     d.nu = y->nu;
+    d.near2 = (float)(y->r_near * y->r_near);
     StageDesc &g = p->stage_host[s];
     g.partial = d.partial;
     g.nchunks = d.nchunks;
@@ -190,8 +200,15 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     g.vol = y->vol.p;
     g.pos32 = y->pos32.p;
     g.vor32 = y->vor32.p;
+    g.poslo = y->poslo.p;
+    g.vorlo = y->vorlo.p;
     g.pos64 = y->pos64.p;
     g.vor64 = y->vor64.p;
+    g.boxes = p->boxes.p + box_off[s];
+    g.box_tile = TB;
+    g.ox = y->ox;
+    g.oy = y->oy;
+    g.oz = y->oz;
     g.dt = 0.0;
     for (int l0 = 0; l0 < d.n; l0 += kStageThreads) sih.push_back(StageItem{(int)s, l0});
   }
@@ -210,8 +227,11 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
   PAWAN_CUDA(ctx, cudaMemcpyAsync(p->stage_descs.p, p->stage_host.data(),
                                   p->stage_host.size() * sizeof(StageDesc), cudaMemcpyHostToDevice,
                                   ctx->stream));
-  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   out = std::move(p);
+  // the plan's tile boxes: repack the current states (idempotent for the
+  // packed arrays, which already hold pack(X) between API calls)
+  PAWAN_TRY(launch_stage_mode(ctx, *out, STAGE_PACK));
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return PAWAN_OK;
 }
 
@@ -247,6 +267,12 @@ static cudaEvent_t take_event(pawan_ctx *ctx) {
 }
 
 int launch_pairs(pawan_ctx *ctx, Plan &p, bool allow_events) {
+  for (size_t s = 0; s < p.systems.size(); ++s)
+    if (p.box_versions[s] != p.systems[s]->pack_version) {
+      // another plan repacked these systems since this plan's boxes were made
+      PAWAN_TRY(launch_stage_mode(ctx, p, STAGE_PACK));
+      break;
+    }
   PAWAN_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(int), ctx->stream));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (ctx->profile && allow_events) {
@@ -276,11 +302,18 @@ int launch_pairs(pawan_ctx *ctx, Plan &p, bool allow_events) {
   return PAWAN_OK;
 }
 
+static void note_repack(Plan &p) {
+  for (size_t s = 0; s < p.systems.size(); ++s) {
+    p.systems[s]->pack_version++;
+    p.box_versions[s] = p.systems[s]->pack_version;
+  }
+}
+
 int launch_stage_mode(pawan_ctx *ctx, Plan &p, int mode) {
-  cudaError_t e = launch_stage(mode, PACK_F32 | PACK_F64, p.n_stage_blocks, p.stage_items.p,
-                               p.stage_descs.p, ctx->stream);
+  cudaError_t e = launch_stage(mode, p.n_stage_blocks, p.stage_items.p, p.stage_descs.p, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "stage kernel launch");
   ctx->launches++;
+  if (mode != STAGE_RATES) note_repack(p);
   return PAWAN_OK;
 }
 
@@ -299,6 +332,11 @@ int rk4_steps(pawan_ctx *ctx, Plan &p, size_t nsteps, bool use_graph) {
     return PAWAN_OK;
   }
   if (!p.graph_exec) {
+    for (size_t s = 0; s < p.systems.size(); ++s)
+      if (p.box_versions[s] != p.systems[s]->pack_version) {
+        PAWAN_TRY(launch_stage_mode(ctx, p, STAGE_PACK));
+        break;
+      }
     PAWAN_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
     const unsigned long long before = ctx->launches.load();
     int st = rk4_one_step(ctx, p, false);
@@ -314,8 +352,14 @@ int rk4_steps(pawan_ctx *ctx, Plan &p, size_t nsteps, bool use_graph) {
     PAWAN_CUDA(ctx, cudaGraphInstantiate(&p.graph_exec, g, 0));
   }
   for (size_t k = 0; k < nsteps; ++k) {
+    for (size_t s = 0; s < p.systems.size(); ++s)
+      if (p.box_versions[s] != p.systems[s]->pack_version) {
+        PAWAN_TRY(launch_stage_mode(ctx, p, STAGE_PACK));
+        break;
+      }
     PAWAN_CUDA(ctx, cudaGraphLaunch(p.graph_exec, ctx->stream));
     ctx->launches += 8;
+    for (int st = 0; st < 4; ++st) note_repack(p);
   }
   return PAWAN_OK;
 }
@@ -384,6 +428,8 @@ int system_alloc(pawan_system *sys) {
   PAWAN_CUDA(ctx, sys->wake_id.alloc(n));
   PAWAN_CUDA(ctx, sys->pos32.alloc(n));
   PAWAN_CUDA(ctx, sys->vor32.alloc(n));
+  PAWAN_CUDA(ctx, sys->poslo.alloc(n));
+  PAWAN_CUDA(ctx, sys->vorlo.alloc(n));
   PAWAN_CUDA(ctx, sys->pos64.alloc(n));
   PAWAN_CUDA(ctx, sys->vor64.alloc(n));
   PAWAN_CUDA(ctx, sys->diag_scratch.alloc(diag_scratch_doubles((int)n)));
@@ -441,7 +487,8 @@ int state_from_device(pawan_system *sys, const double *dev_union, double *state)
 
 size_t pawan_system::device_bytes() const {
   return X.bytes() + Xs.bytes() + K1.bytes() + K2.bytes() + R.bytes() + rad.bytes() +
-         vol.bytes() + wake_id.bytes() + pos32.bytes() + vor32.bytes() + pos64.bytes() +
+         vol.bytes() + wake_id.bytes() + pos32.bytes() + vor32.bytes() + poslo.bytes() +
+         vorlo.bytes() + pos64.bytes() +
          vor64.bytes() + diag_scratch.bytes() + diag_out.bytes() +
          (plan ? plan->partial.bytes() : 0);
 }
@@ -456,6 +503,28 @@ size_t pawan_system::device_bytes() const {
 static int pack_after_state(pawan_system *sys) {
   PAWAN_TRY(system_ensure_plan(sys));
   return launch_stage_mode(sys->ctx, *sys->plan, STAGE_PACK);
+}
+
+// Origin of the FP32 positions (centroid) and the near-tile radius: tile pairs
+// closer than max(4 s_max, 0.03 * extent) use the hi/lo pair formulation.
+static void set_geometry(pawan_system *sys, const double *pos, const double *rad) {
+  const size_t N = sys->n;
+  double c[3] = {0, 0, 0};
+  for (size_t i = 0; i < N; ++i)
+    for (int k = 0; k < 3; ++k) c[k] += pos[3 * i + k];
+  for (int k = 0; k < 3; ++k) c[k] /= (double)N;
+  double ext2 = 0, smax = 0;
+  for (size_t i = 0; i < N; ++i) {
+    double r2 = 0;
+    for (int k = 0; k < 3; ++k) r2 += (pos[3 * i + k] - c[k]) * (pos[3 * i + k] - c[k]);
+    ext2 = std::max(ext2, r2);
+    smax = std::max(smax, rad[i]);
+  }
+  sys->ox = c[0];
+  sys->oy = c[1];
+  sys->oz = c[2];
+  sys->r_near = std::max(4.0 * smax, 0.03 * std::sqrt(ext2));
+  sys->geometry_version++;
 }
 
 extern "C" {
@@ -648,9 +717,10 @@ int pawan_system_create(pawan_ctx *ctx, size_t n_wakes, const size_t *num_partic
   return PAWAN_OK;
 }
 
+// Device buffers are released with cudaFree, which waits for outstanding
+// work on them; the context is not touched, so a system may outlive it.
 void pawan_system_destroy(pawan_system *sys) {
   if (!sys) return;
-  if (sys->ctx) cudaStreamSynchronize(sys->ctx->stream);
   delete sys;
 }
 
@@ -667,6 +737,10 @@ int pawan_system_set_particles(pawan_system *sys, const double *position, const 
   for (size_t i = 0; i < N; ++i)
     if (!(radius[i] > 0.0) || !std::isfinite(radius[i]))
       return fail(ctx, PAWAN_ERR_INVALID, "smoothing radii must be positive");
+  for (size_t i = 0; i < 3 * N; ++i)
+    if (!std::isfinite(position[i]) || !std::isfinite(vorticity[i]))
+      return fail(ctx, PAWAN_ERR_INVALID, "non-finite position or vorticity");
+  set_geometry(sys, position, radius);
   PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->X.p, position, 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->X.p + 3 * N, vorticity, 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->rad.p, radius, N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
@@ -901,7 +975,6 @@ int pawan_batch_create(pawan_ctx *ctx, size_t n, pawan_system *const *systems, p
 
 void pawan_batch_destroy(pawan_batch *b) {
   if (!b) return;
-  cudaStreamSynchronize(b->ctx->stream);
   delete b;
 }
 

@@ -97,10 +97,14 @@ struct pawan_system {
   pawan::TileChoice tile;
   pawan::DBuf<double> X, Xs, K1, K2, R, rad, vol, diag_scratch, diag_out;
   pawan::DBuf<int> wake_id;
-  pawan::DBuf<float4> pos32, vor32;
+  pawan::DBuf<float4> pos32, vor32, poslo, vorlo;
   pawan::DBuf<double4> pos64, vor64;
   std::unique_ptr<pawan::Plan> plan;  // single-system plan for `tile`
-  double dt_uploaded = -1.0;
+  // origin of the FP32 positions and near-tile radius, fixed by set_particles
+  double ox = 0, oy = 0, oz = 0;
+  double r_near = 0;
+  unsigned long long geometry_version = 0;  // bumps when origin / r_near change
+  unsigned long long pack_version = 0;      // bumps whenever the packed arrays change
   size_t device_bytes() const;
 };
 
@@ -111,6 +115,8 @@ namespace pawan {
 struct Plan {
   std::vector<pawan_system *> systems;
   std::vector<double> nus;  // nu of each system when the plan was built
+  std::vector<unsigned long long> geometry_versions;
+  std::vector<unsigned long long> box_versions;  // pack_version the boxes were made at
   int precision = PAWAN_PREC_F32;
   TileChoice tile;
   bool diffusion = false;
@@ -120,6 +126,7 @@ struct Plan {
   double interactions = 0.0;  // sum n^2
   std::vector<int> nchunks;
   DBuf<double> partial;
+  DBuf<float4> boxes;
   DBuf<WorkItem> items;
   DBuf<SegDesc> segs;
   DBuf<StageItem> stage_items;

@@ -57,7 +57,7 @@ struct Request {
 // Device bytes a request holds while active: the system's buffers plus its
 // partial chunks in a batched plan (fixed chunk size).
 double request_bytes(size_t n, int tb) {
-  const double per = 5 * 48.0 + 16.0 + 4.0 + 32.0 + 64.0;
+  const double per = 5 * 48.0 + 16.0 + 4.0 + 64.0 + 64.0 + 1.0;
   const size_t chunk = ((kServeChunkSources + tb - 1) / tb) * (size_t)tb;
   const size_t nch = (n + chunk - 1) / chunk;
   return (double)n * per + 48.0 * (double)n * (double)nch + 4096.0;

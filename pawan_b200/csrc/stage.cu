@@ -1,8 +1,8 @@
 // Per-particle stage kernel: reduces the pair kernel's partial chunks in fixed
 // chunk order into the rates (u | dalpha), applies the RK4 stage update in
-// FP64 with the reference's operation order, and packs the new state into the
-// FP32 / FP64 tile arrays the next pair launch reads.  One thread per particle,
-// HBM-bound.
+// FP64 with the reference's operation order, packs the new state into the
+// FP32 hi/lo and FP64 tile arrays the next pair launch reads, and writes the
+// bounding box of each source tile.  One thread per particle, HBM-bound.
 //
 // Reference: __rk4::step (src/integration/rk4.cpp:12-76):
 //   x1 = k1*(0.5 dt) + x        (:29-31)      STAGE_K1
@@ -18,27 +18,63 @@
 namespace pawan {
 namespace {
 
-__device__ __forceinline__ void pack(const StageDesc &d, int l, const double x[6], int flags) {
+// Packs one particle: FP32 hi/lo pairs of the position relative to the
+// system's origin and of the strength, plus the FP64 copies.  Returns the hi
+// position for the tile's bounding box.
+__device__ __forceinline__ float3 pack(const StageDesc &d, int l, const double x[6]) {
   const double s = d.rad[l];
   const double v = d.vol[l];
-  if (flags & PACK_F32) {
-    d.pos32[l] = make_float4((float)x[0], (float)x[1], (float)x[2], (float)(0.5 * s * s));
-    d.vor32[l] = make_float4((float)x[3], (float)x[4], (float)x[5], (float)v);
+  const double rx = x[0] - d.ox, ry = x[1] - d.oy, rz = x[2] - d.oz;
+  const float hx = (float)rx, hy = (float)ry, hz = (float)rz;
+  const float ax = (float)x[3], ay = (float)x[4], az = (float)x[5];
+  d.pos32[l] = make_float4(hx, hy, hz, (float)(0.5 * s * s));
+  d.poslo[l] = make_float4((float)(rx - (double)hx), (float)(ry - (double)hy),
+                           (float)(rz - (double)hz), 0.f);
+  d.vor32[l] = make_float4(ax, ay, az, (float)v);
+  d.vorlo[l] = make_float4((float)(x[3] - (double)ax), (float)(x[4] - (double)ay),
+                           (float)(x[5] - (double)az), 0.f);
+  d.pos64[l] = make_double4(x[0], x[1], x[2], s);
+  d.vor64[l] = make_double4(x[3], x[4], x[5], v);
+  return make_float3(hx, hy, hz);
+}
+
+// Bounding boxes of the block's tiles (box_tile particles each, aligned to
+// the segment); particles beyond n contribute nothing.
+__device__ __forceinline__ void tile_boxes(const StageDesc &d, int l0, float3 p, bool has) {
+  __shared__ float lo[3][kStageThreads];
+  __shared__ float hi[3][kStageThreads];
+  const int t = threadIdx.x;
+  lo[0][t] = has ? p.x : INFINITY;
+  lo[1][t] = has ? p.y : INFINITY;
+  lo[2][t] = has ? p.z : INFINITY;
+  hi[0][t] = has ? p.x : -INFINITY;
+  hi[1][t] = has ? p.y : -INFINITY;
+  hi[2][t] = has ? p.z : -INFINITY;
+  __syncthreads();
+  for (int s = d.box_tile / 2; s > 0; s >>= 1) {
+    if ((t % d.box_tile) < s) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        lo[k][t] = fminf(lo[k][t], lo[k][t + s]);
+        hi[k][t] = fmaxf(hi[k][t], hi[k][t + s]);
+      }
+    }
+    __syncthreads();
   }
-  if (flags & PACK_F64) {
-    d.pos64[l] = make_double4(x[0], x[1], x[2], s);
-    d.vor64[l] = make_double4(x[3], x[4], x[5], v);
+  if ((t % d.box_tile) == 0 && l0 + t < d.n) {
+    const int b = (l0 + t) / d.box_tile;
+    d.boxes[2 * b] = make_float4(lo[0][t], lo[1][t], lo[2][t], 0.f);
+    d.boxes[2 * b + 1] = make_float4(hi[0][t], hi[1][t], hi[2][t], 0.f);
   }
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(kStageThreads)
-    stage_kernel(const StageItem *__restrict__ items, const StageDesc *__restrict__ descs,
-                 int pack_flags) {
+    stage_kernel(const StageItem *__restrict__ items, const StageDesc *__restrict__ descs) {
   const StageItem it = items[blockIdx.x];
   const StageDesc d = descs[it.seg];
   const int l = it.l0 + threadIdx.x;
-  if (l >= d.n) return;
+  const bool has = l < d.n;
   const size_t n = (size_t)d.n;
   size_t idx[6];
 #pragma unroll
@@ -47,8 +83,8 @@ __global__ void __launch_bounds__(kStageThreads)
     idx[3 + k] = 3 * n + 3 * (size_t)l + k;
   }
 
-  double r[6];
-  if (MODE != STAGE_PACK) {
+  double r[6] = {0, 0, 0, 0, 0, 0};
+  if (MODE != STAGE_PACK && has) {
 #pragma unroll
     for (int k = 0; k < 6; ++k) r[k] = d.partial[(size_t)k * n + l];
     for (int c = 1; c < d.nchunks; ++c) {
@@ -66,74 +102,81 @@ __global__ void __launch_bounds__(kStageThreads)
   const double sixth = dt / 6.;
   const double third = dt / 3.;
 
-  double x[6];
   if (MODE == STAGE_RATES) {
+    if (has) {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) d.R[idx[k]] = r[k];
-    return;
-  } else if (MODE == STAGE_K1 || MODE == STAGE_K2) {
-    double *K = (MODE == STAGE_K1) ? d.K1 : d.K2;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      K[idx[k]] = r[k];
-      x[k] = __dadd_rn(__dmul_rn(r[k], half), d.X[idx[k]]);
-      d.Xs[idx[k]] = x[k];
+      for (int k = 0; k < 6; ++k) d.R[idx[k]] = r[k];
     }
-  } else if (MODE == STAGE_K3) {
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      d.K2[idx[k]] = __dadd_rn(d.K2[idx[k]], r[k]);
-      x[k] = __dadd_rn(__dmul_rn(r[k], full), d.X[idx[k]]);
-      d.Xs[idx[k]] = x[k];
-    }
-  } else if (MODE == STAGE_FINAL) {
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      const double a = __dmul_rn(__dadd_rn(d.K1[idx[k]], r[k]), sixth);
-      const double b = __dmul_rn(d.K2[idx[k]], third);
-      x[k] = __dadd_rn(d.X[idx[k]], __dadd_rn(a, b));
-      d.X[idx[k]] = x[k];
-    }
-  } else if (MODE == STAGE_EULER) {
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-      x[k] = __dadd_rn(d.X[idx[k]], __dmul_rn(r[k], full));
-      d.X[idx[k]] = x[k];
-    }
-  } else {  // STAGE_PACK
-#pragma unroll
-    for (int k = 0; k < 6; ++k) x[k] = d.X[idx[k]];
+    return;  // uniform across the block: no pack, no boxes
   }
-  pack(d, l, x, pack_flags);
+  double x[6] = {0, 0, 0, 0, 0, 0};
+  if (has) {
+    if (MODE == STAGE_K1 || MODE == STAGE_K2) {
+      double *K = (MODE == STAGE_K1) ? d.K1 : d.K2;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        K[idx[k]] = r[k];
+        x[k] = __dadd_rn(__dmul_rn(r[k], half), d.X[idx[k]]);
+        d.Xs[idx[k]] = x[k];
+      }
+    } else if (MODE == STAGE_K3) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        d.K2[idx[k]] = __dadd_rn(d.K2[idx[k]], r[k]);
+        x[k] = __dadd_rn(__dmul_rn(r[k], full), d.X[idx[k]]);
+        d.Xs[idx[k]] = x[k];
+      }
+    } else if (MODE == STAGE_FINAL) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        const double a = __dmul_rn(__dadd_rn(d.K1[idx[k]], r[k]), sixth);
+        const double b = __dmul_rn(d.K2[idx[k]], third);
+        x[k] = __dadd_rn(d.X[idx[k]], __dadd_rn(a, b));
+        d.X[idx[k]] = x[k];
+      }
+    } else if (MODE == STAGE_EULER) {
+#pragma unroll
+      for (int k = 0; k < 6; ++k) {
+        x[k] = __dadd_rn(d.X[idx[k]], __dmul_rn(r[k], full));
+        d.X[idx[k]] = x[k];
+      }
+    } else {  // STAGE_PACK
+#pragma unroll
+      for (int k = 0; k < 6; ++k) x[k] = d.X[idx[k]];
+    }
+  }
+  float3 p = make_float3(0.f, 0.f, 0.f);
+  if (has) p = pack(d, l, x);
+  tile_boxes(d, it.l0, p, has);
 }
 
 }  // namespace
 
-cudaError_t launch_stage(int mode, int pack_flags, int n_blocks, const StageItem *items,
-                         const StageDesc *descs, cudaStream_t s) {
+cudaError_t launch_stage(int mode, int n_blocks, const StageItem *items, const StageDesc *descs,
+                         cudaStream_t s) {
   if (n_blocks <= 0) return cudaSuccess;
   dim3 grid(n_blocks), block(kStageThreads);
   switch (mode) {
     case STAGE_RATES:
-      stage_kernel<STAGE_RATES><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      stage_kernel<STAGE_RATES><<<grid, block, 0, s>>>(items, descs);
       break;
     case STAGE_K1:
-      stage_kernel<STAGE_K1><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      stage_kernel<STAGE_K1><<<grid, block, 0, s>>>(items, descs);
       break;
     case STAGE_K2:
-      stage_kernel<STAGE_K2><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      stage_kernel<STAGE_K2><<<grid, block, 0, s>>>(items, descs);
       break;
     case STAGE_K3:
-      stage_kernel<STAGE_K3><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      stage_kernel<STAGE_K3><<<grid, block, 0, s>>>(items, descs);
       break;
     case STAGE_FINAL:
-      stage_kernel<STAGE_FINAL><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      stage_kernel<STAGE_FINAL><<<grid, block, 0, s>>>(items, descs);
       break;
     case STAGE_EULER:
-      stage_kernel<STAGE_EULER><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      stage_kernel<STAGE_EULER><<<grid, block, 0, s>>>(items, descs);
       break;
     case STAGE_PACK:
-      stage_kernel<STAGE_PACK><<<grid, block, 0, s>>>(items, descs, pack_flags);
+      stage_kernel<STAGE_PACK><<<grid, block, 0, s>>>(items, descs);
       break;
     default:
       return cudaErrorInvalidValue;

@@ -1,0 +1,82 @@
+/* Drop-in GPU interaction for pawan.
+ *
+ * pawan::__cuda is a sibling of the reference's OpenMP class pawan::__parallel
+ * (src/interaction/parallel.h:20-145): same constructors (one or two wakes,
+ * more through addWake), same __system / __interaction interface, so the
+ * reference's integrators (__integration, __rk4) drive it unchanged.  The
+ * all-pairs interaction of every solve() runs on a B200 through the C ABI in
+ * include/pawan_b200.h; results land in each wake's _velocity and _retvorcity
+ * exactly where the reference's interact() puts them, so getRates() and the
+ * rest of the reference code see no difference.
+ *
+ * pawan::__cuda_rk4 is a drop-in for __rk4 (src/integration/rk4.h:14-42): given
+ * a __cuda system it runs whole RK4 steps on the device (state uploaded once
+ * per step, the four stages and their updates in HBM, state read back once);
+ * given any other __system it is the reference __rk4.
+ *
+ * Compile these two files inside the reference tree (they include its
+ * headers) and link libpawan_b200.so.
+ */
+#ifndef PAWAN_B200_DROPIN_CUDA_INTERACTION_H
+#define PAWAN_B200_DROPIN_CUDA_INTERACTION_H
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "pawan_b200.h"
+#include "src/integration/rk4.h"
+#include "src/interaction/interaction.h"
+#include "src/wake/wake.h"
+
+namespace pawan {
+
+class __cuda : public __interaction {
+ public:
+  /* nu defaults to the reference's hard-coded 2.5e-3 (interaction.cpp:13). */
+  explicit __cuda(__wake *W, double nu = 2.5e-3, int precision = PAWAN_PREC_F32, int device = 0);
+  __cuda(__wake *W1, __wake *W2, double nu = 2.5e-3, int precision = PAWAN_PREC_F32,
+         int device = 0);
+  ~__cuda();
+
+  void addWake(__wake *W) override;
+  /* diagnose() of the reference (interaction.cpp:49-93), FP64 on the GPU; fills
+   * the same members and prints the same lines. */
+  void diagnose() override;
+
+  double kineticEnergy();
+  void setViscosity(double nu);
+  /* Uploads the wakes' current positions and vorticities (and, the first time
+   * or after addWake, radii and volumes). */
+  void upload();
+  /* Copies the device state back into the wakes' _position / _vorticity. */
+  void download();
+  pawan_system *device_system() { return _sys; }
+
+ protected:
+  /* The whole-solve hook (interaction.h:106): every wake pair in one launch. */
+  void interact() override;
+
+ private:
+  std::vector<__wake *> _wakes;
+  pawan_ctx *_ctx = nullptr;
+  pawan_system *_sys = nullptr;
+  int _precision;
+  int _device;
+  bool _particles_uploaded = false;
+  void ensure_system();
+  void check(int status, const char *what) const;
+};
+
+class __cuda_rk4 : public __rk4 {
+ public:
+  __cuda_rk4(const double &t, const size_t &n) : __rk4(t, n) {}
+  ~__cuda_rk4() = default;
+
+ protected:
+  void step(const double &dt, __system *S, gsl_vector *state) override;
+};
+
+}  // namespace pawan
+
+#endif
