@@ -58,17 +58,25 @@ def parse():
 # ------------------------------------------------------------------ ranks
 
 class Ranks:
-    def __init__(self, gpus: int):
+    """One process per GPU (torchrun env).  NCCL for the timing reductions; the
+    multi-rank tests run the same code over gloo on CPU (PAWAN_BENCH_BACKEND)."""
+
+    def __init__(self, gpus: int, backend: str = None):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.backend = backend or os.environ.get("PAWAN_BENCH_BACKEND", "nccl")
         self.dist = None
         if self.world > 1:
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                    device_id=torch.device("cuda", self.local))
+            timeout = datetime.timedelta(seconds=120)
+            if self.backend == "nccl":
+                torch.cuda.set_device(self.local)
+                dist.init_process_group("nccl", timeout=timeout,
+                                        device_id=torch.device("cuda", self.local))
+            else:
+                dist.init_process_group(self.backend, timeout=timeout)
             self.dist = dist
             self.torch = torch
 
@@ -79,13 +87,19 @@ class Ranks:
     def max(self, v: float) -> float:
         if not self.dist:
             return v
-        t = self.torch.tensor([v], dtype=self.torch.float64, device=f"cuda:{self.local}")
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = self.torch.tensor([v], dtype=self.torch.float64, device=dev)
         self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
         return float(t.item())
 
     def close(self):
         if self.dist:
             self.dist.destroy_process_group()
+
+
+def aggregate_rate(world: int, interactions_per_rank: float, ms_max: float) -> float:
+    """Whole-job G interactions/s: every rank's work over the slowest rank's time."""
+    return world * interactions_per_rank / (ms_max * 1e-3) / 1e9
 
 
 # ----------------------------------------------------------------- clocks
@@ -257,8 +271,7 @@ def run_pawan(args, rk: Ranks):
     clk = clocks.stop()
     rk.barrier()
     ms_max = rk.max(ms)
-    total_inter = rk.world * 4.0 * N * N * args.steps
-    value = total_inter / (ms_max * 1e-3) / 1e9
+    value = aggregate_rate(rk.world, 4.0 * N * N * args.steps, ms_max)
 
     pair_avg_s = prof["pair_ms"] / max(1, prof["pair_launches"]) * 1e-3
     achieved_tflops = N * N * flops / pair_avg_s / 1e12

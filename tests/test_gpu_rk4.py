@@ -4,7 +4,7 @@ through the C ABI.
 RK4 / Euler: compared on the state increments (final - initial), which is where
 the integrator's arithmetic shows; FP64 paths to 1e-11 RMS, FP32 pair math to
 the FP32 tolerance.  Diagnostics in FP64 against the reference's diagnose().
-Drift: over the full single-ring run (N = 2,048, 200 steps, dt = 0.01) the
+Drift: over the stable first 100 steps of the single-ring run (N = 2,048, dt = 0.01) the
 conserved quantities of the FP32 trajectory stay within stated bounds of the
 FP64 trajectory's.
 """
