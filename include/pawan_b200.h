@@ -203,6 +203,26 @@ int pawan_server_fetch(pawan_server *srv, long long id, double *state, size_t si
 int pawan_server_cancel(pawan_server *srv, long long id);
 int pawan_server_stats(pawan_server *srv, pawan_serve_stats *out);
 
+/* ------------------------------------------------- allocation-free solve */
+/* No counterpart in the reference.  For callers that must not allocate device
+ * memory -- inside someone else's stream capture or host callback, under an
+ * allocator that owns the whole device, or in a latency-critical loop where
+ * cudaMalloc's implicit synchronisation is not acceptable.  One FP32 solve
+ * (all pairs over the n particles, as pawan_system_solve with
+ * PAWAN_PREC_F32) from caller-owned DEVICE arrays: position and vorticity
+ * n x 3, radius and volume n; writes velocity and vorticity rate (n x 3,
+ * device).  All working memory is one static device array reserved by every
+ * GPU that loads the library (about 4.2 MB), so n <= PAWAN_NOALLOC_MAX_PARTICLES;
+ * larger n returns PAWAN_ERR_INVALID.  The first call on a device resolves that
+ * array's address (make it before any stream capture).  Calls share the
+ * array: calls that may overlap on the GPU must be serialised by the caller.
+ * `stream` is a cudaStream_t (NULL: the default stream); the call is
+ * asynchronous on it and allocates nothing. */
+#define PAWAN_NOALLOC_MAX_PARTICLES 16384
+int pawan_interact_noalloc(const double *position, const double *vorticity, const double *radius,
+                           const double *volume, size_t n, double nu, double *velocity,
+                           double *retvorcity, void *stream);
+
 /* ----------------------------------------------------- throughput probes */
 /* Measured FP32 FFMA / FP64 DFMA throughput of the device, GFLOP/s (FMA = 2
  * flops), over `seconds` of back-to-back probe launches. */

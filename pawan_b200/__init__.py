@@ -115,6 +115,9 @@ _SIGS = {
     "pawan_server_fetch": (ctypes.c_int, [_vp, ctypes.c_longlong, _dp, ctypes.c_size_t, _dp, _dp, _dp]),
     "pawan_server_cancel": (ctypes.c_int, [_vp, ctypes.c_longlong]),
     "pawan_server_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ServeStats)]),
+    "pawan_interact_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.c_size_t, ctypes.c_double, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_void_p]),
     "pawan_peak_fp32": (ctypes.c_int, [_vp, ctypes.c_double, _dp]),
     "pawan_peak_fp64": (ctypes.c_int, [_vp, ctypes.c_double, _dp]),
 }
@@ -490,6 +493,19 @@ class Server:
         if st != OK:
             raise PawanError(st, "stats")
         return {f: getattr(s, f) for f, _ in ServeStats._fields_}
+
+
+NOALLOC_MAX_PARTICLES = 16384
+
+
+def interact_noalloc(position: int, vorticity: int, radius: int, volume: int, n: int, nu: float,
+                     velocity: int, retvorcity: int, stream: int = 0) -> int:
+    """The allocation-free solve on caller-owned device arrays (addresses as
+    ints: n x 3 / n float64 inputs, n x 3 float64 outputs).  Returns the C
+    status (0 = ok); asynchronous on `stream` (0: default stream)."""
+    lib = load_library()
+    return int(lib.pawan_interact_noalloc(position, vorticity, radius, volume, int(n), float(nu),
+                                          velocity, retvorcity, stream or None))
 
 
 def union_to_state(counts: Sequence[int], pos: np.ndarray, vor: np.ndarray) -> np.ndarray:

@@ -31,10 +31,11 @@ COMMON = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-Wall",
                  "-I" + INCLUDE, "-I" + CSRC]
 PER_FILE = {
     "pair_f32.cu": ["--ftz=true"],
+    "noalloc.cu": ["--ftz=true"],
     "pair_plain.cu": ["--fmad=false"],
 }
 SOURCES = ["pair_f32.cu", "pair_f64.cu", "pair_plain.cu", "stage.cu", "diag.cu", "peak.cu",
-           "runtime.cpp", "serve.cpp"]
+           "runtime.cpp", "serve.cpp", "noalloc.cu"]
 
 
 def nvcc() -> str:
