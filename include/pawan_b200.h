@@ -43,6 +43,18 @@ extern "C" {
 #define PAWAN_PREC_F64 1        /* FP64, same algebra as the FP32 kernel */
 #define PAWAN_PREC_F64_PLAIN 2  /* FP64, the reference's formula term by term */
 
+/* Tiling of the pair kernel (the compiled variants are listed by
+ * pawan_system_autotune's candidates; set_tiling rejects others). */
+typedef struct {
+  int threads;            /* threads per block = sources per shared-memory tile: 128 or 256 */
+  int threads_per_target; /* threads sharing one target's sources: 1, 2 or 4 */
+  int targets_per_thread; /* targets per thread: 1 or 2 */
+  int unroll;             /* unroll depth of the source loop */
+  int blocks_per_sm;      /* blocks per SM the registers are bounded for, 0 = default */
+  int items_per_slot;     /* work items per resident block (source chunking) */
+  int packed;             /* 1: far tiles two sources per FP32x2 instruction */
+} pawan_tiling;
+
 typedef struct pawan_ctx pawan_ctx;
 typedef struct pawan_system pawan_system;
 typedef struct pawan_batch pawan_batch;
@@ -127,13 +139,9 @@ int pawan_system_set_precision(pawan_system *sys, int precision);
  * radius (N f64): __integration::integrate's per-step output
  * (integration.cpp:20-21, 28-29; interaction.cpp:197-202; wake.cpp:68-73). */
 int pawan_system_write_frame(pawan_system *sys, const char *path, double t, int append);
-/* Pair-kernel tiling: threads per block, threads per target, unroll depth,
- * work items per SM slot.  set_config fixes it; autotune measures the
- * candidates on this system and keeps the fastest. */
-int pawan_system_set_config(pawan_system *sys, int threads, int threads_per_target, int unroll,
-                            int items_per_slot);
-int pawan_system_get_config(pawan_system *sys, int *threads, int *threads_per_target,
-                            int *unroll, int *items_per_slot);
+int pawan_system_set_tiling(pawan_system *sys, const pawan_tiling *tiling);
+int pawan_system_get_tiling(pawan_system *sys, pawan_tiling *tiling);
+/* Times every compiled tiling on this system and keeps the fastest. */
 int pawan_system_autotune(pawan_system *sys);
 /* Device address of the state [x | alpha] in union layout (6N doubles,
  * x = first 3N) for callers that keep data on the device. */
@@ -152,8 +160,7 @@ void pawan_batch_destroy(pawan_batch *batch);
 int pawan_batch_rk4(pawan_batch *batch, const double *dt, double dt0, size_t nsteps,
                     int use_graph);
 int pawan_batch_solve(pawan_batch *batch);
-int pawan_batch_set_config(pawan_batch *batch, int threads, int threads_per_target, int unroll,
-                           int items_per_slot);
+int pawan_batch_set_tiling(pawan_batch *batch, const pawan_tiling *tiling);
 int pawan_batch_autotune(pawan_batch *batch);
 
 /* ---------------------------------------------------------------- serving */
@@ -224,8 +231,9 @@ int pawan_interact_noalloc(const double *position, const double *vorticity, cons
                            double *retvorcity, void *stream);
 
 /* ----------------------------------------------------- throughput probes */
-/* Measured FP32 FFMA / FP64 DFMA throughput of the device, GFLOP/s (FMA = 2
- * flops), over `seconds` of back-to-back probe launches. */
+/* Measured FP32 / FP64 FMA throughput of the device, GFLOP/s (FMA = 2
+ * flops), over `seconds` of back-to-back probe launches.  The FP32 figure is
+ * the larger of scalar FFMA and packed FP32x2 FFMA2 chains. */
 int pawan_peak_fp32(pawan_ctx *ctx, double seconds, double *gflops);
 int pawan_peak_fp64(pawan_ctx *ctx, double seconds, double *gflops);
 

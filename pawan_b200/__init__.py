@@ -53,6 +53,18 @@ class ServeConfig(ctypes.Structure):
                 ("precision", ctypes.c_int)]
 
 
+class Tiling(ctypes.Structure):
+    _fields_ = [("threads", ctypes.c_int), ("threads_per_target", ctypes.c_int),
+                ("targets_per_thread", ctypes.c_int), ("unroll", ctypes.c_int),
+                ("blocks_per_sm", ctypes.c_int), ("items_per_slot", ctypes.c_int), ("packed", ctypes.c_int)]
+
+
+def _tiling(threads, threads_per_target=1, unroll=4, items_per_slot=16, targets_per_thread=1,
+            blocks_per_sm=0, packed=False) -> Tiling:
+    return Tiling(threads, threads_per_target, targets_per_thread, unroll, blocks_per_sm, items_per_slot,
+                  1 if packed else 0)
+
+
 class ServeStats(ctypes.Structure):
     _fields_ = [("submitted", ctypes.c_ulonglong), ("admitted", ctypes.c_ulonglong),
                 ("completed", ctypes.c_ulonglong), ("rejected", ctypes.c_ulonglong),
@@ -96,15 +108,15 @@ _SIGS = {
     "pawan_system_set_nu": (ctypes.c_int, [_vp, ctypes.c_double]),
     "pawan_system_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pawan_system_write_frame": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_double, ctypes.c_int]),
-    "pawan_system_set_config": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
-    "pawan_system_get_config": (ctypes.c_int, [_vp] + [ctypes.POINTER(ctypes.c_int)] * 4),
+    "pawan_system_set_tiling": (ctypes.c_int, [_vp, ctypes.POINTER(Tiling)]),
+    "pawan_system_get_tiling": (ctypes.c_int, [_vp, ctypes.POINTER(Tiling)]),
     "pawan_system_autotune": (ctypes.c_int, [_vp]),
     "pawan_system_device_state": (ctypes.c_int, [_vp, ctypes.POINTER(_dp)]),
     "pawan_batch_create": (ctypes.c_int, [_vp, ctypes.c_size_t, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "pawan_batch_destroy": (None, [_vp]),
     "pawan_batch_rk4": (ctypes.c_int, [_vp, _dp, ctypes.c_double, ctypes.c_size_t, ctypes.c_int]),
     "pawan_batch_solve": (ctypes.c_int, [_vp]),
-    "pawan_batch_set_config": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "pawan_batch_set_tiling": (ctypes.c_int, [_vp, ctypes.POINTER(Tiling)]),
     "pawan_batch_autotune": (ctypes.c_int, [_vp]),
     "pawan_server_create": (ctypes.c_int, [_vp, ctypes.POINTER(ServeConfig), ctypes.POINTER(_vp)]),
     "pawan_server_destroy": (None, [_vp]),
@@ -356,14 +368,17 @@ class System:
         self.ctx.check(self._lib.pawan_system_write_frame(self._h, os.fsencode(path), float(t),
                                                           1 if append else 0))
 
-    def set_config(self, threads: int, threads_per_target: int, unroll: int, items_per_slot: int = 16):
-        self.ctx.check(self._lib.pawan_system_set_config(self._h, threads, threads_per_target, unroll,
-                                                         items_per_slot))
+    def set_config(self, threads: int, threads_per_target: int = 1, unroll: int = 4,
+                   items_per_slot: int = 16, targets_per_thread: int = 1, blocks_per_sm: int = 0,
+                   packed: bool = False):
+        t = _tiling(threads, threads_per_target, unroll, items_per_slot, targets_per_thread, blocks_per_sm,
+                    packed)
+        self.ctx.check(self._lib.pawan_system_set_tiling(self._h, ctypes.byref(t)))
 
     def get_config(self) -> dict:
-        v = [ctypes.c_int() for _ in range(4)]
-        self.ctx.check(self._lib.pawan_system_get_config(self._h, *[ctypes.byref(x) for x in v]))
-        return dict(zip(("threads", "threads_per_target", "unroll", "items_per_slot"), [x.value for x in v]))
+        t = Tiling()
+        self.ctx.check(self._lib.pawan_system_get_tiling(self._h, ctypes.byref(t)))
+        return {f: getattr(t, f) for f, _ in Tiling._fields_}
 
     def autotune(self) -> dict:
         self.ctx.check(self._lib.pawan_system_autotune(self._h))
@@ -404,9 +419,12 @@ class Batch:
     def solve(self):
         self.ctx.check(self._lib.pawan_batch_solve(self._h))
 
-    def set_config(self, threads: int, threads_per_target: int, unroll: int, items_per_slot: int = 16):
-        self.ctx.check(self._lib.pawan_batch_set_config(self._h, threads, threads_per_target, unroll,
-                                                        items_per_slot))
+    def set_config(self, threads: int, threads_per_target: int = 1, unroll: int = 4,
+                   items_per_slot: int = 16, targets_per_thread: int = 1, blocks_per_sm: int = 0,
+                   packed: bool = False):
+        t = _tiling(threads, threads_per_target, unroll, items_per_slot, targets_per_thread, blocks_per_sm,
+                    packed)
+        self.ctx.check(self._lib.pawan_batch_set_tiling(self._h, ctypes.byref(t)))
 
     def autotune(self):
         self.ctx.check(self._lib.pawan_batch_autotune(self._h))

@@ -8,15 +8,20 @@
 namespace pawan {
 
 // Tiling of the all-pairs kernels: `tb` threads per block (= sources per
-// shared-memory tile), `p` threads per target (targets per block = tb / p),
-// `unroll` = unroll depth of the source loop.
+// shared-memory tile), `p` threads per target, `r` targets per thread
+// (targets per block = tb / p * r), `unroll` = unroll depth of the source loop,
+// `minb` = blocks per SM the registers are bounded for (0: the default),
+// `packed` = far tiles computed two sources per FP32x2 instruction.
 struct PairConfig {
   int tb;
   int p;
   int unroll;
+  int r = 1;
+  int minb = 0;
+  bool packed = false;
 };
 
-inline int targets_per_block(const PairConfig &c) { return c.tb / c.p; }
+inline int targets_per_block(const PairConfig &c) { return c.tb / c.p * c.r; }
 
 // FP32 pair math, FP64 accumulation of per-tile partial sums.
 bool pairs_f32_supported(const PairConfig &c);
@@ -52,6 +57,8 @@ cudaError_t launch_diagnostics(int n, const double4 *pos64, const double4 *vor64
 // Throughput probes: FP32 FFMA and FP64 DFMA chains.  flops = launched FMAs * 2.
 cudaError_t launch_ffma_peak(int blocks, int threads, int iters, float *sink, cudaStream_t s);
 cudaError_t launch_dfma_peak(int blocks, int threads, int iters, double *sink, cudaStream_t s);
+// FMAs launched: as above (kPeakChains FMAs per thread and repetition, in pairs).
+cudaError_t launch_ffma2_peak(int blocks, int threads, int iters, float *sink, cudaStream_t s);
 constexpr int kPeakChains = 8;
 
 }  // namespace pawan

@@ -83,51 +83,145 @@ __device__ __forceinline__ void load_source(const SegDesc &sg, int j, int s1, fl
   }
 }
 
-template <bool DIFF, int P, int NSRC, int U>
+// q, F and the diffusion factor of one pair in units of A = 1/(4 pi), from
+// sigma^2, w = (rho^2 + sigma^2)^-1/2 and ri = 1/rho (u = sigma^2 w^2):
+//   Dp = (u w)^5 = sigma^10 w^15,  Zc = Dp sigma^2,
+//   ph = (rho^2 + 1.5 sigma^2) w^4 / rho = (1 + u/2) w^2 / rho,
+//   qh = (ph - 7.5 Zc) sigma^2 / rho^2,   fh = (2.5 Zc - qh) / rho^2.
+// 16 FP32 instructions.
+__device__ __forceinline__ void kernel_scalars(float sig2, float w, float ri, float &qh, float &fh,
+                                               float &dp) {
+  const float w2 = w * w;
+  const float uu = sig2 * w2;
+  const float v = uu * w;
+  const float v2 = v * v;
+  const float v4 = v2 * v2;
+  dp = v4 * v;
+  const float zc = dp * sig2;
+  const float ph = fmaf(0.5f, uu, 1.0f) * w2 * ri;
+  const float ri2 = ri * ri;
+  qh = fmaf(-7.5f, zc, ph) * sig2 * ri2;
+  fh = fmaf(2.5f, zc, -qh) * ri2;
+}
+
+template <bool DIFF, int P, int R, int NSRC, int U>
 __device__ __forceinline__ void tile_far(const float4 *__restrict__ sp,
-                                         const float4 *__restrict__ sv, int g, const Target &T,
-                                         Acc32 &a) {
+                                         const float4 *__restrict__ sv, int g,
+                                         const Target (&T)[R], Acc32 (&a)[R]) {
 #pragma unroll U
   for (int k = 0; k < NSRC / P; ++k) {
     const int jj = g + P * k;
     const float4 p = sp[jj];
     const float4 s = sv[jj];
-    const float dx = T.xh - p.x, dy = T.yh - p.y, dz = T.zh - p.z;
-    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-    const float sig2 = T.h + p.w;
-    const float w = rsqrtf(r2 + sig2);
-    const float ri = rsqrtf(r2);
-    const float ri2 = ri * ri;
-    const float w2 = w * w;
-    const float w4 = w2 * w2;
-    const float uu = sig2 * w2;
-    const float u2 = uu * uu;
-    const float u4 = u2 * u2;
-    const float u5 = u4 * uu;
-    const float dp = u5 * (w4 * w);
-    const float zc = dp * sig2;
-    const float ph = fmaf(1.5f, sig2, r2) * w4 * ri;
-    const float qh = fmaf(-7.5f, zc, ph) * sig2 * ri2;
-    const float fh = fmaf(2.5f, zc, -qh) * ri2;
-    const float cx = fmaf(s.y, dz, -s.z * dy);
-    const float cy = fmaf(s.z, dx, -s.x * dz);
-    const float cz = fmaf(s.x, dy, -s.y * dx);
-    const float t = fmaf(T.ch, cz, fmaf(T.bh, cy, T.ah * cx));
-    const float ft = fh * t;
-    a.ux = fmaf(qh, cx, a.ux);
-    a.uy = fmaf(qh, cy, a.uy);
-    a.uz = fmaf(qh, cz, a.uz);
-    a.qx = fmaf(qh, s.x, a.qx);
-    a.qy = fmaf(qh, s.y, a.qy);
-    a.qz = fmaf(qh, s.z, a.qz);
-    a.gx = fmaf(ft, dx, a.gx);
-    a.gy = fmaf(ft, dy, a.gy);
-    a.gz = fmaf(ft, dz, a.gz);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const float dx = T[r].xh - p.x, dy = T[r].yh - p.y, dz = T[r].zh - p.z;
+      const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      const float sig2 = T[r].h + p.w;
+      const float w = rsqrtf(r2 + sig2);
+      const float ri = rsqrtf(r2);
+      float qh, fh, dp;
+      kernel_scalars(sig2, w, ri, qh, fh, dp);
+      const float cx = fmaf(s.y, dz, -s.z * dy);
+      const float cy = fmaf(s.z, dx, -s.x * dz);
+      const float cz = fmaf(s.x, dy, -s.y * dx);
+      const float t = fmaf(T[r].ch, cz, fmaf(T[r].bh, cy, T[r].ah * cx));
+      const float ft = fh * t;
+      a[r].ux = fmaf(qh, cx, a[r].ux);
+      a[r].uy = fmaf(qh, cy, a[r].uy);
+      a[r].uz = fmaf(qh, cz, a[r].uz);
+      a[r].qx = fmaf(qh, s.x, a[r].qx);
+      a[r].qy = fmaf(qh, s.y, a[r].qy);
+      a[r].qz = fmaf(qh, s.z, a[r].qz);
+      a[r].gx = fmaf(ft, dx, a[r].gx);
+      a[r].gy = fmaf(ft, dy, a[r].gy);
+      a[r].gz = fmaf(ft, dz, a[r].gz);
+      if (DIFF) {
+        a[r].ex = fmaf(dp, s.x, a[r].ex);
+        a[r].ey = fmaf(dp, s.y, a[r].ey);
+        a[r].ez = fmaf(dp, s.z, a[r].ez);
+        a[r].ev = fmaf(dp, s.w, a[r].ev);
+      }
+    }
+  }
+}
+
+// ---- packed far path: two sources per FP32x2 instruction -----------------
+// Shared-memory layout of a source tile for it, per source pair k = (2k, 2k+1):
+//   f0[k] = (-x_2k, -x_2k+1, -y_2k, -y_2k+1)   f1[k] = (-z_2k, -z_2k+1, h_2k, h_2k+1)
+//   f2[k] = (ax_2k, ax_2k+1, ay_2k, ay_2k+1)   f3[k] = (az_2k, az_2k+1, v_2k, v_2k+1)
+// so a float4 load yields two operand pairs and the target enters every
+// instruction as a broadcast pair held in registers.
+
+struct Acc2 {
+  float2 ux, uy, uz;
+  float2 qx, qy, qz;  // sum -qh alpha_j   (signs folded into the per-tile fold)
+  float2 gx, gy, gz;
+  float2 ex, ey, ez;
+  float2 ev;
+};
+
+struct Target2 {
+  float2 x, y, z, h;  // broadcast (value, value)
+  float2 a, b, c;     // strength hi, broadcast
+};
+
+__device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 neg2(float2 v) { return make_float2(-v.x, -v.y); }
+
+template <bool DIFF, int NSRC, int U>
+__device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
+                                                const float4 *__restrict__ f1,
+                                                const float4 *__restrict__ f2,
+                                                const float4 *__restrict__ f3, const Target2 &T,
+                                                Acc2 &a) {
+#pragma unroll U
+  for (int k = 0; k < NSRC / 2; ++k) {
+    const float4 A0 = f0[k], A1 = f1[k], A2 = f2[k], A3 = f3[k];
+    const float2 npx = make_float2(A0.x, A0.y), npy = make_float2(A0.z, A0.w);
+    const float2 npz = make_float2(A1.x, A1.y), hj = make_float2(A1.z, A1.w);
+    const float2 sx = make_float2(A2.x, A2.y), sy = make_float2(A2.z, A2.w);
+    const float2 sz = make_float2(A3.x, A3.y), sv = make_float2(A3.z, A3.w);
+    const float2 dx = __fadd2_rn(T.x, npx);
+    const float2 dy = __fadd2_rn(T.y, npy);
+    const float2 dz = __fadd2_rn(T.z, npz);
+    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+    const float2 sig2 = __fadd2_rn(T.h, hj);
+    const float2 sr = __fadd2_rn(r2, sig2);
+    const float2 w = make_float2(rsqrtf(sr.x), rsqrtf(sr.y));
+    const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    // kernel_scalars() in pairs, with qn = -qh
+    const float2 w2 = __fmul2_rn(w, w);
+    const float2 uu = __fmul2_rn(sig2, w2);
+    const float2 vv = __fmul2_rn(uu, w);
+    const float2 v2 = __fmul2_rn(vv, vv);
+    const float2 v4 = __fmul2_rn(v2, v2);
+    const float2 dp = __fmul2_rn(v4, vv);
+    const float2 zc = __fmul2_rn(dp, sig2);
+    const float2 nph = __fmul2_rn(__fmul2_rn(__ffma2_rn(bc2(-0.5f), uu, bc2(-1.0f)), w2), ri);
+    const float2 ri2 = __fmul2_rn(ri, ri);
+    const float2 qn = __fmul2_rn(__fmul2_rn(__ffma2_rn(bc2(7.5f), zc, nph), sig2), ri2);
+    const float2 fh = __fmul2_rn(__ffma2_rn(bc2(2.5f), zc, qn), ri2);
+    // c = alpha_j x d
+    const float2 cx = __ffma2_rn(sy, dz, neg2(__fmul2_rn(sz, dy)));
+    const float2 cy = __ffma2_rn(sz, dx, neg2(__fmul2_rn(sx, dz)));
+    const float2 cz = __ffma2_rn(sx, dy, neg2(__fmul2_rn(sy, dx)));
+    const float2 t = __ffma2_rn(T.c, cz, __ffma2_rn(T.b, cy, __fmul2_rn(T.a, cx)));
+    const float2 ft = __fmul2_rn(fh, t);
+    a.ux = __ffma2_rn(qn, cx, a.ux);
+    a.uy = __ffma2_rn(qn, cy, a.uy);
+    a.uz = __ffma2_rn(qn, cz, a.uz);
+    a.qx = __ffma2_rn(qn, sx, a.qx);
+    a.qy = __ffma2_rn(qn, sy, a.qy);
+    a.qz = __ffma2_rn(qn, sz, a.qz);
+    a.gx = __ffma2_rn(ft, dx, a.gx);
+    a.gy = __ffma2_rn(ft, dy, a.gy);
+    a.gz = __ffma2_rn(ft, dz, a.gz);
     if (DIFF) {
-      a.ex = fmaf(dp, s.x, a.ex);
-      a.ey = fmaf(dp, s.y, a.ey);
-      a.ez = fmaf(dp, s.z, a.ez);
-      a.ev = fmaf(dp, s.w, a.ev);
+      a.ex = __ffma2_rn(dp, sx, a.ex);
+      a.ey = __ffma2_rn(dp, sy, a.ey);
+      a.ez = __ffma2_rn(dp, sz, a.ez);
+      a.ev = __ffma2_rn(dp, sv, a.ev);
     }
   }
 }
@@ -152,73 +246,68 @@ __device__ __forceinline__ void cross_accurate(float ax, float ay, float az, flo
   wz = det2(ax, ay, bx, by) + fmaf(ax, my, fmaf(-ay, mx, fmaf(lx, by, -ly * bx)));
 }
 
-template <bool DIFF, bool CHECK, int P, int NSRC, int U>
+template <bool DIFF, bool CHECK, int P, int R, int NSRC>
 __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
                                           const float4 *__restrict__ sv,
                                           const float4 *__restrict__ spl,
-                                          const float4 *__restrict__ svl, int g, int skip,
-                                          const Target &T, Acc32 &a) {
-  // near tiles are a few percent of the work: a shallow unroll keeps the
-  // register budget of the far loop
-#pragma unroll(U < 2 ? U : 2)
+                                          const float4 *__restrict__ svl, int g,
+                                          const int (&skip)[R], const Target (&T)[R],
+                                          Acc32 (&a)[R]) {
+  // near tiles are a few percent of the work: no unrolling keeps the register
+  // budget of the far loop
+#pragma unroll 1
   for (int k = 0; k < NSRC / P; ++k) {
     const int jj = g + P * k;
     const float4 p = sp[jj];
     const float4 s = sv[jj];
     const float4 pl = spl[jj];
     const float4 sl = svl[jj];
-    const float dx = (T.xh - p.x) + (T.xl - pl.x);
-    const float dy = (T.yh - p.y) + (T.yl - pl.y);
-    const float dz = (T.zh - p.z) + (T.zl - pl.z);
-    const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-    const float sig2 = T.h + p.w;
-    const float w = rsqrtf(r2 + sig2);
-    const float ri = rsqrtf(r2);
-    const float ri2 = ri * ri;
-    const float w2 = w * w;
-    const float w4 = w2 * w2;
-    const float uu = sig2 * w2;
-    const float u2 = uu * uu;
-    const float u4 = u2 * u2;
-    const float u5 = u4 * uu;
-    float dp = u5 * (w4 * w);
-    const float zc = dp * sig2;
-    const float ph = fmaf(1.5f, sig2, r2) * w4 * ri;
-    float qh = fmaf(-7.5f, zc, ph) * sig2 * ri2;
-    const float fh = fmaf(2.5f, zc, -qh) * ri2;
-    // velocity: alpha_j x d
-    const float cx = fmaf(s.y, dz, -s.z * dy);
-    const float cy = fmaf(s.z, dx, -s.x * dz);
-    const float cz = fmaf(s.x, dy, -s.y * dx);
-    // stretching: alpha_i x alpha_j from the hi/lo strengths
-    float wx, wy, wz;
-    cross_accurate(T.ah, T.bh, T.ch, T.al, T.bl, T.cl, s.x, s.y, s.z, sl.x, sl.y, sl.z, wx, wy, wz);
-    const float t = fmaf(dz, wz, fmaf(dy, wy, dx * wx));
-    float ft = fh * t;
-    if (CHECK) {
-      const bool self = (jj == skip);
-      qh = self ? 0.f : qh;
-      ft = self ? 0.f : ft;
-      dp = self ? 0.f : dp;
-    }
-    a.ux = fmaf(qh, cx, a.ux);
-    a.uy = fmaf(qh, cy, a.uy);
-    a.uz = fmaf(qh, cz, a.uz);
-    a.qx = fmaf(qh, wx, a.qx);
-    a.qy = fmaf(qh, wy, a.qy);
-    a.qz = fmaf(qh, wz, a.qz);
-    a.gx = fmaf(ft, dx, a.gx);
-    a.gy = fmaf(ft, dy, a.gy);
-    a.gz = fmaf(ft, dz, a.gz);
-    if (DIFF) {
-      // delta = alpha_j - alpha_i from the hi/lo strengths
-      const float ex = (s.x - T.ah) + (sl.x - T.al);
-      const float ey = (s.y - T.bh) + (sl.y - T.bl);
-      const float ez = (s.z - T.ch) + (sl.z - T.cl);
-      a.ex = fmaf(dp, ex, a.ex);
-      a.ey = fmaf(dp, ey, a.ey);
-      a.ez = fmaf(dp, ez, a.ez);
-      a.ev = fmaf(dp, T.v - s.w, a.ev);
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const float dx = (T[r].xh - p.x) + (T[r].xl - pl.x);
+      const float dy = (T[r].yh - p.y) + (T[r].yl - pl.y);
+      const float dz = (T[r].zh - p.z) + (T[r].zl - pl.z);
+      const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+      const float sig2 = T[r].h + p.w;
+      const float w = rsqrtf(r2 + sig2);
+      const float ri = rsqrtf(r2);
+      float qh, fh, dp;
+      kernel_scalars(sig2, w, ri, qh, fh, dp);
+      // velocity: alpha_j x d
+      const float cx = fmaf(s.y, dz, -s.z * dy);
+      const float cy = fmaf(s.z, dx, -s.x * dz);
+      const float cz = fmaf(s.x, dy, -s.y * dx);
+      // stretching: alpha_i x alpha_j from the hi/lo strengths
+      float wx, wy, wz;
+      cross_accurate(T[r].ah, T[r].bh, T[r].ch, T[r].al, T[r].bl, T[r].cl, s.x, s.y, s.z, sl.x, sl.y,
+                     sl.z, wx, wy, wz);
+      const float t = fmaf(dz, wz, fmaf(dy, wy, dx * wx));
+      float ft = fh * t;
+      if (CHECK) {
+        const bool self = (jj == skip[r]);
+        qh = self ? 0.f : qh;
+        ft = self ? 0.f : ft;
+        dp = self ? 0.f : dp;
+      }
+      a[r].ux = fmaf(qh, cx, a[r].ux);
+      a[r].uy = fmaf(qh, cy, a[r].uy);
+      a[r].uz = fmaf(qh, cz, a[r].uz);
+      a[r].qx = fmaf(qh, wx, a[r].qx);
+      a[r].qy = fmaf(qh, wy, a[r].qy);
+      a[r].qz = fmaf(qh, wz, a[r].qz);
+      a[r].gx = fmaf(ft, dx, a[r].gx);
+      a[r].gy = fmaf(ft, dy, a[r].gy);
+      a[r].gz = fmaf(ft, dz, a[r].gz);
+      if (DIFF) {
+        // delta = alpha_j - alpha_i from the hi/lo strengths
+        const float ex = (s.x - T[r].ah) + (sl.x - T[r].al);
+        const float ey = (s.y - T[r].bh) + (sl.y - T[r].bl);
+        const float ez = (s.z - T[r].ch) + (sl.z - T[r].cl);
+        a[r].ex = fmaf(dp, ex, a[r].ex);
+        a[r].ey = fmaf(dp, ey, a[r].ey);
+        a[r].ez = fmaf(dp, ez, a[r].ez);
+        a[r].ev = fmaf(dp, T[r].v - s.w, a[r].ev);
+      }
     }
   }
 }
@@ -230,19 +319,28 @@ __device__ __forceinline__ float box_gap2(float4 alo, float4 ahi, float4 blo, fl
   return gx * gx + gy * gy + gz * gz;
 }
 
-template <int TB, int P, int U, bool DIFF>
-__global__ void __launch_bounds__(TB, (TB <= 128 ? 4 : 2))
+// Threads per target P > 1 split a tile's sources (R = 1); targets per thread
+// R > 1 reuse each source loaded from shared memory for R targets (P = 1);
+// PK: the far path processes two sources per FP32x2 instruction (P = R = 1).
+// MINB: blocks per SM the register allocation is bounded for (occupancy).
+template <int TB, int P, int R, int U, bool DIFF, int MINB, bool PK>
+__global__ void __launch_bounds__(TB, MINB)
     pairs_f32_kernel(const WorkItem *__restrict__ items, int n_items,
                      const SegDesc *__restrict__ segs, int *__restrict__ next_item) {
-  constexpr int TPB = TB / P;
+  static_assert(!PK || (P == 1 && R == 1), "the packed far path has one target per thread");
+  constexpr int TG = TB / P;   // targets per block and per target row r
+  constexpr int TPB = TG * R;  // targets per block
+  constexpr int FQ = PK ? TB / 2 : 1;
   __shared__ float4 sp[2][TB];
   __shared__ float4 sv[2][TB];
   __shared__ float4 spl[2][TB];
   __shared__ float4 svl[2][TB];
+  __shared__ float4 fq[4][2][FQ];
   __shared__ int s_item;
   const int tid = threadIdx.x;
   const int g = tid % P;
   const int lt = tid / P;
+  const double A = kInv4Pi;
 
   for (;;) {
     if (tid == 0) s_item = atomicAdd(next_item, 1);
@@ -253,103 +351,182 @@ __global__ void __launch_bounds__(TB, (TB <= 128 ? 4 : 2))
 
     const WorkItem w = items[it];
     const SegDesc sg = segs[w.seg];
-    const int i = w.t0 + lt;
-    const bool valid = i < sg.n;
-    Target T;
-    {
+    const double cnu = 15.0 * sg.nu * A;
+    int ti[R];
+    bool valid[R];
+    Target T[R];
+    double ax[R], ay[R], az[R];
+    double ou[R][3], oa[R][3];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      ti[r] = w.t0 + lt + r * TG;
+      valid[r] = ti[r] < sg.n;
       float4 a = make_float4(0.f, 0.f, 0.f, 1.f), b = make_float4(0.f, 0.f, 0.f, 0.f);
       float4 c = b, d = b;
-      if (valid) {
-        a = __ldg(sg.pos32 + i);
-        b = __ldg(sg.vor32 + i);
-        c = __ldg(sg.poslo + i);
-        d = __ldg(sg.vorlo + i);
+      if (valid[r]) {
+        a = __ldg(sg.pos32 + ti[r]);
+        b = __ldg(sg.vor32 + ti[r]);
+        c = __ldg(sg.poslo + ti[r]);
+        d = __ldg(sg.vorlo + ti[r]);
       }
-      T.xh = a.x; T.yh = a.y; T.zh = a.z; T.h = a.w;
-      T.ah = b.x; T.bh = b.y; T.ch = b.z; T.v = b.w;
-      T.xl = c.x; T.yl = c.y; T.zl = c.z;
-      T.al = d.x; T.bl = d.y; T.cl = d.z;
+      T[r].xh = a.x; T[r].yh = a.y; T[r].zh = a.z; T[r].h = a.w;
+      T[r].ah = b.x; T[r].bh = b.y; T[r].ch = b.z; T[r].v = b.w;
+      T[r].xl = c.x; T[r].yl = c.y; T[r].zl = c.z;
+      T[r].al = d.x; T[r].bl = d.y; T[r].cl = d.z;
+      // target strength in FP64 (hi + lo) for the per-tile folds
+      ax[r] = (double)T[r].ah + (double)T[r].al;
+      ay[r] = (double)T[r].bh + (double)T[r].bl;
+      az[r] = (double)T[r].ch + (double)T[r].cl;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) ou[r][k] = oa[r][k] = 0.0;
     }
-    // target strength in FP64 (hi + lo) for the per-tile folds
-    const double ax = (double)T.ah + (double)T.al;
-    const double ay = (double)T.bh + (double)T.bl;
-    const double az = (double)T.ch + (double)T.cl;
-    const double A = kInv4Pi;
-    const double cnu = 15.0 * sg.nu * A;
-    double ou0 = 0, ou1 = 0, ou2 = 0, oa0 = 0, oa1 = 0, oa2 = 0;
 
-    // the target tile lies inside source tile t0 / TB (TPB divides TB)
-    const float4 tlo = __ldg(sg.boxes + 2 * (w.t0 / TB));
-    const float4 thi = __ldg(sg.boxes + 2 * (w.t0 / TB) + 1);
+    Target2 T2;
+    if (PK) {
+      T2.x = bc2(T[0].xh);
+      T2.y = bc2(T[0].yh);
+      T2.z = bc2(T[0].zh);
+      T2.h = bc2(T[0].h);
+      T2.a = bc2(T[0].ah);
+      T2.b = bc2(T[0].bh);
+      T2.c = bc2(T[0].ch);
+    }
+
+    // box of the target tile: union of the source-tile boxes it covers
+    float4 tlo = __ldg(sg.boxes + 2 * (w.t0 / TB));
+    float4 thi = __ldg(sg.boxes + 2 * (w.t0 / TB) + 1);
+#pragma unroll
+    for (int q = 1; q < (TPB + TB - 1) / TB; ++q) {
+      if (w.t0 + q * TB < sg.n) {
+        const float4 l2 = __ldg(sg.boxes + 2 * (w.t0 / TB + q));
+        const float4 h2 = __ldg(sg.boxes + 2 * (w.t0 / TB + q) + 1);
+        tlo = make_float4(fminf(tlo.x, l2.x), fminf(tlo.y, l2.y), fminf(tlo.z, l2.z), 0.f);
+        thi = make_float4(fmaxf(thi.x, h2.x), fmaxf(thi.y, h2.y), fmaxf(thi.z, h2.z), 0.f);
+      }
+    }
 
     const int ntiles = (w.s1 - w.s0 + TB - 1) / TB;
-    float4 r[4];
-    load_source(sg, w.s0 + tid, w.s1, r);
+    float4 rs[4];
+    load_source(sg, w.s0 + tid, w.s1, rs);
     for (int t = 0; t < ntiles; ++t) {
       const int buf = t & 1;
-      sp[buf][tid] = r[0];
-      sv[buf][tid] = r[1];
-      spl[buf][tid] = r[2];
-      svl[buf][tid] = r[3];
+      sp[buf][tid] = rs[0];
+      sv[buf][tid] = rs[1];
+      spl[buf][tid] = rs[2];
+      svl[buf][tid] = rs[3];
+      if (PK) {
+        const int k = tid >> 1, hf = tid & 1;
+        float *q0 = reinterpret_cast<float *>(&fq[0][buf][k]);
+        float *q1 = reinterpret_cast<float *>(&fq[1][buf][k]);
+        float *q2 = reinterpret_cast<float *>(&fq[2][buf][k]);
+        float *q3 = reinterpret_cast<float *>(&fq[3][buf][k]);
+        q0[hf] = -rs[0].x;
+        q0[2 + hf] = -rs[0].y;
+        q1[hf] = -rs[0].z;
+        q1[2 + hf] = rs[0].w;
+        q2[hf] = rs[1].x;
+        q2[2 + hf] = rs[1].y;
+        q3[hf] = rs[1].z;
+        q3[2 + hf] = rs[1].w;
+      }
       __syncthreads();
       const int ts = w.s0 + t * TB;
-      if (t + 1 < ntiles) load_source(sg, ts + TB + tid, w.s1, r);
-      Acc32 a = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (t + 1 < ntiles) load_source(sg, ts + TB + tid, w.s1, rs);
+      Acc32 a[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) a[r] = Acc32{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       const bool diag = (ts < w.t0 + TPB) && (w.t0 < ts + TB);
       const float4 slo = __ldg(sg.boxes + 2 * (ts / TB));
       const float4 shi = __ldg(sg.boxes + 2 * (ts / TB) + 1);
       const bool near = diag || box_gap2(tlo, thi, slo, shi) < sg.near2;
       if (!near) {
-        tile_far<DIFF, P, TB, U>(sp[buf], sv[buf], g, T, a);
-        const double Qx = A * a.qx, Qy = A * a.qy, Qz = A * a.qz;
-        oa0 += (ay * Qz - az * Qy) + 3.0 * A * a.gx;
-        oa1 += (az * Qx - ax * Qz) + 3.0 * A * a.gy;
-        oa2 += (ax * Qy - ay * Qx) + 3.0 * A * a.gz;
-        if (DIFF) {
-          oa0 += cnu * ((double)T.v * a.ex - (double)a.ev * ax);
-          oa1 += cnu * ((double)T.v * a.ey - (double)a.ev * ay);
-          oa2 += cnu * ((double)T.v * a.ez - (double)a.ev * az);
+        if (PK) {
+          Acc2 b;
+          b.ux = b.uy = b.uz = b.qx = b.qy = b.qz = b.gx = b.gy = b.gz = make_float2(0.f, 0.f);
+          b.ex = b.ey = b.ez = b.ev = make_float2(0.f, 0.f);
+          tile_far_packed<DIFF, TB, U>(fq[0][buf], fq[1][buf], fq[2][buf], fq[3][buf], T2, b);
+          a[0].ux = -(b.ux.x + b.ux.y);
+          a[0].uy = -(b.uy.x + b.uy.y);
+          a[0].uz = -(b.uz.x + b.uz.y);
+          a[0].qx = -(b.qx.x + b.qx.y);
+          a[0].qy = -(b.qy.x + b.qy.y);
+          a[0].qz = -(b.qz.x + b.qz.y);
+          a[0].gx = b.gx.x + b.gx.y;
+          a[0].gy = b.gy.x + b.gy.y;
+          a[0].gz = b.gz.x + b.gz.y;
+          a[0].ex = b.ex.x + b.ex.y;
+          a[0].ey = b.ey.x + b.ey.y;
+          a[0].ez = b.ez.x + b.ez.y;
+          a[0].ev = b.ev.x + b.ev.y;
+        } else {
+          tile_far<DIFF, P, R, TB, U>(sp[buf], sv[buf], g, T, a);
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const double Qx = A * a[r].qx, Qy = A * a[r].qy, Qz = A * a[r].qz;
+          oa[r][0] += (ay[r] * Qz - az[r] * Qy) + 3.0 * A * a[r].gx;
+          oa[r][1] += (az[r] * Qx - ax[r] * Qz) + 3.0 * A * a[r].gy;
+          oa[r][2] += (ax[r] * Qy - ay[r] * Qx) + 3.0 * A * a[r].gz;
+          if (DIFF) {
+            const double v = T[r].v;
+            oa[r][0] += cnu * (v * a[r].ex - (double)a[r].ev * ax[r]);
+            oa[r][1] += cnu * (v * a[r].ey - (double)a[r].ev * ay[r]);
+            oa[r][2] += cnu * (v * a[r].ez - (double)a[r].ev * az[r]);
+          }
         }
       } else {
+        int skip[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) skip[r] = ti[r] - ts;
         if (diag)
-          tile_near<DIFF, true, P, TB, U>(sp[buf], sv[buf], spl[buf], svl[buf], g, i - ts, T, a);
+          tile_near<DIFF, true, P, R, TB>(sp[buf], sv[buf], spl[buf], svl[buf], g, skip, T, a);
         else
-          tile_near<DIFF, false, P, TB, U>(sp[buf], sv[buf], spl[buf], svl[buf], g, -1, T, a);
-        oa0 += A * a.qx + 3.0 * A * a.gx;
-        oa1 += A * a.qy + 3.0 * A * a.gy;
-        oa2 += A * a.qz + 3.0 * A * a.gz;
-        if (DIFF) {
-          oa0 += cnu * ((double)T.v * a.ex + (double)a.ev * ax);
-          oa1 += cnu * ((double)T.v * a.ey + (double)a.ev * ay);
-          oa2 += cnu * ((double)T.v * a.ez + (double)a.ev * az);
+          tile_near<DIFF, false, P, R, TB>(sp[buf], sv[buf], spl[buf], svl[buf], g, skip, T, a);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          oa[r][0] += A * a[r].qx + 3.0 * A * a[r].gx;
+          oa[r][1] += A * a[r].qy + 3.0 * A * a[r].gy;
+          oa[r][2] += A * a[r].qz + 3.0 * A * a[r].gz;
+          if (DIFF) {
+            const double v = T[r].v;
+            oa[r][0] += cnu * (v * a[r].ex + (double)a[r].ev * ax[r]);
+            oa[r][1] += cnu * (v * a[r].ey + (double)a[r].ev * ay[r]);
+            oa[r][2] += cnu * (v * a[r].ez + (double)a[r].ev * az[r]);
+          }
         }
       }
-      ou0 += A * a.ux;
-      ou1 += A * a.uy;
-      ou2 += A * a.uz;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        ou[r][0] += A * a[r].ux;
+        ou[r][1] += A * a[r].uy;
+        ou[r][2] += A * a[r].uz;
+      }
     }
 
     if (P > 1) {
 #pragma unroll
       for (int off = 1; off < P; off <<= 1) {
-        ou0 += __shfl_xor_sync(0xffffffffu, ou0, off);
-        ou1 += __shfl_xor_sync(0xffffffffu, ou1, off);
-        ou2 += __shfl_xor_sync(0xffffffffu, ou2, off);
-        oa0 += __shfl_xor_sync(0xffffffffu, oa0, off);
-        oa1 += __shfl_xor_sync(0xffffffffu, oa1, off);
-        oa2 += __shfl_xor_sync(0xffffffffu, oa2, off);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          ou[0][k] += __shfl_xor_sync(0xffffffffu, ou[0][k], off);
+          oa[0][k] += __shfl_xor_sync(0xffffffffu, oa[0][k], off);
+        }
       }
     }
 
-    if (valid && g == 0) {
+    if (g == 0) {
       const size_t n = (size_t)sg.n;
-      double *out = sg.partial + (size_t)w.chunk * 6 * n + i;
-      out[0] = ou0;
-      out[n] = ou1;
-      out[2 * n] = ou2;
-      out[3 * n] = oa0;
-      out[4 * n] = oa1;
-      out[5 * n] = oa2;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        if (!valid[r]) continue;
+        double *out = sg.partial + (size_t)w.chunk * 6 * n + ti[r];
+        out[0] = ou[r][0];
+        out[n] = ou[r][1];
+        out[2 * n] = ou[r][2];
+        out[3 * n] = oa[r][0];
+        out[4 * n] = oa[r][1];
+        out[5 * n] = oa[r][2];
+      }
     }
   }
 }
@@ -358,21 +535,35 @@ using KernelFn = void (*)(const WorkItem *, int, const SegDesc *, int *);
 
 template <bool DIFF>
 KernelFn select(const PairConfig &c) {
-#define PAWAN_F32_CASE(TB_, P_, U_) \
-  if (c.tb == TB_ && c.p == P_ && c.unroll == U_) return &pairs_f32_kernel<TB_, P_, U_, DIFF>;
-  PAWAN_F32_CASE(128, 1, 2)
-  PAWAN_F32_CASE(128, 1, 4)
-  PAWAN_F32_CASE(128, 2, 2)
-  PAWAN_F32_CASE(128, 2, 4)
-  PAWAN_F32_CASE(128, 4, 2)
-  PAWAN_F32_CASE(128, 4, 4)
-  PAWAN_F32_CASE(256, 1, 2)
-  PAWAN_F32_CASE(256, 1, 4)
-  PAWAN_F32_CASE(256, 2, 2)
-  PAWAN_F32_CASE(256, 2, 4)
-  PAWAN_F32_CASE(256, 4, 2)
-  PAWAN_F32_CASE(256, 4, 4)
+#define PAWAN_F32_CASE_PK(TB_, P_, R_, U_, MINB_, PK_)                                   \
+  if (c.tb == TB_ && c.p == P_ && c.r == R_ && c.unroll == U_ && c.packed == PK_ &&      \
+      (c.minb == MINB_ || (c.minb == 0 && MINB_ == (TB_ <= 128 ? 4 : 2))))              \
+    return &pairs_f32_kernel<TB_, P_, R_, U_, DIFF, MINB_, PK_>;
+#define PAWAN_F32_CASE(TB_, P_, R_, U_, MINB_) PAWAN_F32_CASE_PK(TB_, P_, R_, U_, MINB_, false)
+  PAWAN_F32_CASE_PK(128, 1, 1, 1, 4, true)
+  PAWAN_F32_CASE_PK(128, 1, 1, 2, 4, true)
+  PAWAN_F32_CASE_PK(128, 1, 1, 1, 5, true)
+  PAWAN_F32_CASE_PK(128, 1, 1, 2, 5, true)
+  PAWAN_F32_CASE(128, 1, 1, 2, 4)
+  PAWAN_F32_CASE(128, 1, 1, 4, 4)
+  PAWAN_F32_CASE(128, 2, 1, 2, 4)
+  PAWAN_F32_CASE(128, 2, 1, 4, 4)
+  PAWAN_F32_CASE(128, 4, 1, 4, 4)
+  PAWAN_F32_CASE(128, 1, 2, 1, 4)
+  PAWAN_F32_CASE(128, 1, 2, 2, 4)
+  PAWAN_F32_CASE(128, 1, 1, 2, 5)
+  PAWAN_F32_CASE(128, 1, 1, 4, 5)
+  PAWAN_F32_CASE(128, 1, 1, 2, 6)
+  PAWAN_F32_CASE(128, 1, 1, 4, 6)
+  PAWAN_F32_CASE(256, 1, 1, 2, 2)
+  PAWAN_F32_CASE(256, 1, 1, 4, 2)
+  PAWAN_F32_CASE(256, 2, 1, 4, 2)
+  PAWAN_F32_CASE(256, 4, 1, 4, 2)
+  PAWAN_F32_CASE(256, 1, 2, 1, 2)
+  PAWAN_F32_CASE(256, 1, 2, 2, 2)
+  PAWAN_F32_CASE(256, 1, 1, 4, 3)
 #undef PAWAN_F32_CASE
+#undef PAWAN_F32_CASE_PK
   return nullptr;
 }
 

@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(TB)
 using KernelFn = void (*)(const WorkItem *, int, const SegDesc *, int *);
 
 KernelFn select(const PairConfig &c, bool diffusion) {
-  if (c.p != 1) return nullptr;
+  if (c.p != 1 || c.r != 1) return nullptr;
   if (c.tb == 128) return diffusion ? &pairs_f64_kernel<128, true> : &pairs_f64_kernel<128, false>;
   if (c.tb == 256) return diffusion ? &pairs_f64_kernel<256, true> : &pairs_f64_kernel<256, false>;
   return nullptr;

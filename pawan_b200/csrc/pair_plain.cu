@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(TB)
 using KernelFn = void (*)(const WorkItem *, int, const SegDesc *, int *);
 
 KernelFn select(const PairConfig &c) {
-  if (c.p != 1) return nullptr;
+  if (c.p != 1 || c.r != 1) return nullptr;
   if (c.tb == 128) return &pairs_plain_kernel<128>;
   if (c.tb == 256) return &pairs_plain_kernel<256>;
   return nullptr;

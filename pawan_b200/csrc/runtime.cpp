@@ -37,27 +37,35 @@ int cuda_fail(pawan_ctx *ctx, cudaError_t e, const char *where) {
     if (s_ != PAWAN_OK) return s_;  \
   } while (0)
 
+// Defaults measured on the ring pair and the helical wake (N = 131,072 and
+// 262,144): two targets per thread, 256 threads, shallow unroll, fine chunks.
 TileChoice default_tile(int precision) {
   TileChoice t;
   if (precision == PAWAN_PREC_F32) {
-    t.pc = PairConfig{128, 1, 4};
+    t.pc = PairConfig{256, 1, 1, 2};
   } else {
     t.pc = PairConfig{128, 1, 1};
   }
-  t.items_per_slot = 16;
+  t.items_per_slot = 32;
   return t;
 }
 
 std::vector<TileChoice> tile_candidates(int precision) {
   std::vector<TileChoice> v;
   if (precision == PAWAN_PREC_F32) {
+    // (threads per target, targets per thread, unroll, blocks per SM) as
+    // compiled in pair_f32.cu (0 = the default register bound)
+    // (.., packed) among those compiled in pair_f32.cu: the ones that led on
+    // some workload (threads per target > 1 for small systems, two targets
+    // per thread or packed pairs for large ones)
+    const int shapes[][5] = {{1, 1, 4, 0, 0}, {2, 1, 4, 0, 0}, {4, 1, 4, 0, 0}, {1, 2, 1, 0, 0},
+                             {1, 2, 2, 0, 0}, {1, 1, 4, 5, 0}, {1, 1, 2, 0, 1}, {1, 1, 2, 5, 1}};
     for (int tb : {128, 256})
-      for (int p : {1, 2, 4})
-        for (int u : {2, 4}) {
-          TileChoice t;
-          t.pc = PairConfig{tb, p, u};
-          v.push_back(t);
-        }
+      for (const auto &sh : shapes) {
+        TileChoice t;
+        t.pc = PairConfig{tb, sh[0], sh[2], sh[1], sh[3], sh[4] != 0};
+        if (pairs_f32_supported(t.pc)) v.push_back(t);
+      }
   } else {
     for (int tb : {128, 256}) {
       TileChoice t;
@@ -893,26 +901,38 @@ int pawan_system_write_frame(pawan_system *sys, const char *path, double t, int 
   return PAWAN_OK;
 }
 
-int pawan_system_set_config(pawan_system *sys, int threads, int threads_per_target, int unroll,
-                            int items_per_slot) {
+static int tile_from_abi(pawan_ctx *ctx, int precision, const pawan_tiling *t, TileChoice *out) {
+  if (!t) return fail(ctx, PAWAN_ERR_INVALID, "null tiling");
+  TileChoice c;
+  c.pc = PairConfig{t->threads, t->threads_per_target, t->unroll, t->targets_per_thread,
+                    t->blocks_per_sm, t->packed != 0};
+  c.items_per_slot = t->items_per_slot;
+  if (t->items_per_slot < 1 || t->targets_per_thread < 1 || t->blocks_per_sm < 0 ||
+      !tile_supported(precision, c.pc))
+    return fail(ctx, PAWAN_ERR_INVALID, "tiling not compiled for this precision");
+  *out = c;
+  return PAWAN_OK;
+}
+
+int pawan_system_set_tiling(pawan_system *sys, const pawan_tiling *tiling) {
   CHECK_SYS(sys);
   TileChoice t;
-  t.pc = PairConfig{threads, threads_per_target, unroll};
-  t.items_per_slot = items_per_slot;
-  if (items_per_slot < 1 || !tile_supported(sys->precision, t.pc))
-    return fail(sys->ctx, PAWAN_ERR_INVALID, "unsupported tiling for this precision");
+  PAWAN_TRY(tile_from_abi(sys->ctx, sys->precision, tiling, &t));
   sys->tile = t;
   sys->fixed_tile = true;
   return PAWAN_OK;
 }
 
-int pawan_system_get_config(pawan_system *sys, int *threads, int *threads_per_target, int *unroll,
-                            int *items_per_slot) {
+int pawan_system_get_tiling(pawan_system *sys, pawan_tiling *tiling) {
   CHECK_SYS(sys);
-  if (threads) *threads = sys->tile.pc.tb;
-  if (threads_per_target) *threads_per_target = sys->tile.pc.p;
-  if (unroll) *unroll = sys->tile.pc.unroll;
-  if (items_per_slot) *items_per_slot = sys->tile.items_per_slot;
+  if (!tiling) return PAWAN_ERR_INVALID;
+  tiling->threads = sys->tile.pc.tb;
+  tiling->threads_per_target = sys->tile.pc.p;
+  tiling->targets_per_thread = sys->tile.pc.r;
+  tiling->unroll = sys->tile.pc.unroll;
+  tiling->blocks_per_sm = sys->tile.pc.minb;
+  tiling->packed = sys->tile.pc.packed ? 1 : 0;
+  tiling->items_per_slot = sys->tile.items_per_slot;
   return PAWAN_OK;
 }
 
@@ -992,14 +1012,10 @@ int pawan_batch_solve(pawan_batch *b) {
   return launch_stage_mode(b->ctx, *b->plan, STAGE_RATES);
 }
 
-int pawan_batch_set_config(pawan_batch *b, int threads, int threads_per_target, int unroll,
-                           int items_per_slot) {
+int pawan_batch_set_tiling(pawan_batch *b, const pawan_tiling *tiling) {
   if (!b) return PAWAN_ERR_INVALID;
   TileChoice t;
-  t.pc = PairConfig{threads, threads_per_target, unroll};
-  t.items_per_slot = items_per_slot;
-  if (items_per_slot < 1 || !tile_supported(b->precision, t.pc))
-    return fail(b->ctx, PAWAN_ERR_INVALID, "unsupported tiling for this precision");
+  PAWAN_TRY(tile_from_abi(b->ctx, b->precision, tiling, &t));
   b->tile = t;
   return PAWAN_OK;
 }
@@ -1017,7 +1033,9 @@ int pawan_batch_autotune(pawan_batch *b) {
 
 // ------------------------------------------------------------ throughput
 
-static int run_peak(pawan_ctx *ctx, double seconds, double *gflops, bool fp64) {
+// kind: 0 = FP32 FFMA, 1 = FP64 DFMA, 2 = packed FP32x2 FFMA2
+static int run_peak(pawan_ctx *ctx, double seconds, double *gflops, int kind) {
+  const bool fp64 = kind == 1;
   CHECK_CTX(ctx);
   if (!gflops) return PAWAN_ERR_INVALID;
   const int threads = 256;
@@ -1030,9 +1048,11 @@ static int run_peak(pawan_ctx *ctx, double seconds, double *gflops, bool fp64) {
   PAWAN_CUDA(ctx, cudaEventCreate(&e1));
   auto launch = [&]() -> cudaError_t {
     ctx->launches++;
-    return fp64 ? launch_dfma_peak(blocks, threads, iters, sink.p, ctx->stream)
-                : launch_ffma_peak(blocks, threads, iters, reinterpret_cast<float *>(sink.p),
-                                   ctx->stream);
+    if (kind == 1) return launch_dfma_peak(blocks, threads, iters, sink.p, ctx->stream);
+    if (kind == 2)
+      return launch_ffma2_peak(blocks, threads, iters, reinterpret_cast<float *>(sink.p),
+                               ctx->stream);
+    return launch_ffma_peak(blocks, threads, iters, reinterpret_cast<float *>(sink.p), ctx->stream);
   };
   cudaError_t e = launch();  // warm-up
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -1060,11 +1080,16 @@ static int run_peak(pawan_ctx *ctx, double seconds, double *gflops, bool fp64) {
 }
 
 int pawan_peak_fp32(pawan_ctx *ctx, double seconds, double *gflops) {
-  return run_peak(ctx, seconds, gflops, false);
+  if (!gflops) return PAWAN_ERR_INVALID;
+  double a = 0, b = 0;
+  PAWAN_TRY(run_peak(ctx, 0.5 * seconds, &a, 0));
+  PAWAN_TRY(run_peak(ctx, 0.5 * seconds, &b, 2));
+  *gflops = a > b ? a : b;
+  return PAWAN_OK;
 }
 
 int pawan_peak_fp64(pawan_ctx *ctx, double seconds, double *gflops) {
-  return run_peak(ctx, seconds, gflops, true);
+  return run_peak(ctx, seconds, gflops, 1);
 }
 
 }  // extern "C"

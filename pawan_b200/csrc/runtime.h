@@ -50,7 +50,8 @@ struct TileChoice {
   PairConfig pc{128, 1, 4};
   int items_per_slot = 16;
   bool operator==(const TileChoice &o) const {
-    return pc.tb == o.pc.tb && pc.p == o.pc.p && pc.unroll == o.pc.unroll &&
+    return pc.tb == o.pc.tb && pc.p == o.pc.p && pc.r == o.pc.r && pc.unroll == o.pc.unroll &&
+           pc.minb == o.pc.minb && pc.packed == o.pc.packed &&
            items_per_slot == o.items_per_slot;
   }
 };

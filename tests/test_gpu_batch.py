@@ -74,7 +74,7 @@ def test_system_autotune(ctx):
     sc = g.single_ring(n_stations=128, seed=2, nu=1e-3)
     s = System.from_scenario(ctx, sc, "f32")
     cfg = s.autotune()
-    assert cfg["threads"] in (128, 256) and cfg["threads_per_target"] in (1, 2, 4)
+    assert cfg["threads"] in (128, 256) and cfg["threads_per_target"] in (1, 2, 4) and cfg["targets_per_thread"] in (1, 2)
     s.solve()
     pos, vor, rad, vol = sc.union()
     u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, sc.nu)

@@ -2,7 +2,8 @@
 
 Tolerances (tests/helpers.py): FP32 pair math with FP64 accumulation -- RMS
 relative error <= 1e-5 and max error <= 1e-4 of the max reference value, for
-velocity and vorticity rate separately; FP64 kernels -- RMS <= 1e-12, max <= 1e-11.
+velocity and vorticity rate separately; plain FP64 -- RMS <= 1e-12, max <= 1e-11;
+tuned FP64 -- RMS <= 1e-10, max <= 1e-9.
 """
 import numpy as np
 import pytest
@@ -87,18 +88,43 @@ def test_many_wakes_union(ctx):
     check("f32", *s.union_rates(), u_ref, da_ref)
 
 
-@pytest.mark.parametrize("tb", [128, 256])
-@pytest.mark.parametrize("p", [1, 2, 4])
-@pytest.mark.parametrize("unroll", [2, 4])
-def test_every_f32_tiling(ctx, tb, p, unroll):
+# (threads, threads per target, targets per thread, unroll, blocks per SM) as compiled
+F32_TILINGS = [(128, 1, 1, 2, 0), (128, 1, 1, 4, 0), (128, 2, 1, 2, 0), (128, 2, 1, 4, 0),
+               (128, 4, 1, 4, 0), (128, 1, 2, 1, 0), (128, 1, 2, 2, 0), (128, 1, 1, 2, 5),
+               (128, 1, 1, 4, 5), (128, 1, 1, 2, 6), (128, 1, 1, 4, 6), (256, 1, 1, 2, 0),
+               (256, 1, 1, 4, 0), (256, 2, 1, 4, 0), (256, 4, 1, 4, 0), (256, 1, 2, 1, 0),
+               (256, 1, 2, 2, 0), (256, 1, 1, 4, 3)]
+# packed far path (two sources per FP32x2 instruction): (threads, unroll, blocks per SM)
+F32_PACKED = [(128, 1, 0), (128, 2, 0), (128, 1, 5), (128, 2, 5)]
+
+
+@pytest.mark.parametrize("tb,unroll,minb", F32_PACKED)
+def test_every_packed_f32_tiling(ctx, tb, unroll, minb):
+    sc = g.ring_pair(n_stations=70, seed=34, nu=1e-3)
+    pos, vor, rad, vol = sc.union()
+    s = System.from_scenario(ctx, sc, "f32")
+    for nu in (1e-3, 0.0):
+        s.set_nu(nu)
+        u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, nu)
+        for ips in (1, 16, 64):
+            s.set_config(tb, 1, unroll, ips, blocks_per_sm=minb, packed=True)
+            s.solve()
+            check("f32", *s.union_rates(), u_ref, da_ref)
+
+
+@pytest.mark.parametrize("tb,p,r,unroll,minb", F32_TILINGS)
+def test_every_f32_tiling(ctx, tb, p, r, unroll, minb):
     sc = g.ring_pair(n_stations=70, seed=33, nu=1e-3)  # N = 1120: ragged tiles
     pos, vor, rad, vol = sc.union()
     u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, sc.nu)
     s = System.from_scenario(ctx, sc, "f32")
     for ips in (1, 16, 64):
-        s.set_config(tb, p, unroll, ips)
+        s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb)
         s.solve()
         check("f32", *s.union_rates(), u_ref, da_ref)
+    s.set_nu(0.0)
+    s.solve()
+    check("f32", *s.union_rates(), *oracle.pairs(pos, vor, rad, vol, 0.0))
 
 
 def test_nu_zero_matches_and_set_nu(ctx):
