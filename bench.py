@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--quick", action="store_true",
                     help="main timed loop only (no autotune, FP64 comparison, e2e, CPU baseline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-suite", action="store_true", help="skip the batch and serving legs")
     return ap.parse_args()
 
 
@@ -152,6 +153,16 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows), "power_w_max": max(pw) if pw else None}
 
 
+def gpu_processes(index: int) -> int:
+    """Compute processes nvidia-smi lists on the GPU (other tenants slow a run)."""
+    try:
+        out = subprocess.run(["nvidia-smi", "-i", str(index), "--query-compute-apps=pid",
+                              "--format=csv,noheader"], capture_output=True, text=True, timeout=20).stdout
+        return len([l for l in out.splitlines() if l.strip()])
+    except (OSError, subprocess.SubprocessError):
+        return -1
+
+
 def gpu_index(local: int) -> int:
     vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
     parts = [p for p in vis.split(",") if p.strip()]
@@ -230,6 +241,115 @@ def run_reference(args, rk: Ranks):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------- ragged batch leg
+
+def run_batch_leg(ctx, n_solves: int = 512, steps: int = 4, seed: int = 4) -> dict:
+    """512 independent single-ring solves (N log-uniform in [512, 16384]):
+    `steps` RK4 steps of every solve as one batch (one persistent pair launch
+    per stage, the step captured in a CUDA graph, tiles autotuned), against the
+    same steps run one solve per launch sequence.  solves/s = solves x
+    (steps / 100) per second, a solve being the workload's 100 steps."""
+    from pawan_b200 import Batch, System
+    from pawan_b200 import geometry as g
+    scs = g.ragged_batch(n_solves=n_solves, seed=seed)
+    inter = sum(4.0 * sc.n * sc.n for sc in scs) * steps
+    dt = scs[0].dt
+    batched = [System.from_scenario(ctx, sc, "f32") for sc in scs]
+    b = Batch(ctx, batched)
+    b.autotune()
+    b.rk4(dt, 1, use_graph=True)      # capture + warm-up
+    ctx.synchronize()
+    ctx.mark(2)
+    b.rk4(dt, steps, use_graph=True)
+    ctx.mark(3)
+    t_b = ctx.elapsed_ms(2, 3) * 1e-3
+    b.close()
+    for s in batched:
+        s.close()
+    solo = [System.from_scenario(ctx, sc, "f32") for sc in scs]
+    for s in solo:                    # each with its own plan, default tiling
+        s.rk4(dt, 1)
+    ctx.synchronize()
+    ctx.mark(2)
+    for s in solo:
+        s.rk4(dt, steps)
+    ctx.mark(3)
+    t_s = ctx.elapsed_ms(2, 3) * 1e-3
+    for s in solo:
+        s.close()
+    frac = steps / 100.0
+    return {"solves": n_solves, "steps_timed": steps,
+            "batched": {"solves_per_s": n_solves * frac / t_b, "G_interactions_per_s": inter / t_b / 1e9,
+                        "seconds": t_b},
+            "one_solve_per_launch": {"solves_per_s": n_solves * frac / t_s,
+                                     "G_interactions_per_s": inter / t_s / 1e9, "seconds": t_s},
+            "speedup": t_s / t_b}
+
+
+# -------------------------------------------------------------- serving leg
+
+def run_serving_leg(ctx, rate: float, duration: float, n_lo: int, n_hi: int, steps_lo: int,
+                    steps_hi: int, budget: float, cap: float, max_active: int, max_queue: int,
+                    drain: float, seed: int = 5) -> dict:
+    """Replays a Poisson arrival trace against the continuous-batching server in
+    real time.  Requests are built and submitted at their arrival times; when
+    the server's queue is full an arrival is rejected without building it (the
+    engine would reject it the same way).  After the arrival window the run
+    waits up to `drain` seconds for requests in flight."""
+    from pawan_b200 import Server
+    from pawan_b200 import geometry as g
+    reqs = g.serving_requests(rate=rate, duration=duration, seed=seed, n_lo=n_lo, n_hi=n_hi,
+                              steps_lo=steps_lo, steps_hi=steps_hi, build=False)
+    srv = Server(ctx, budget_bytes=budget, max_step_interactions=cap, max_active=max_active,
+                 max_queue=max_queue)
+    ids, rejected_full, rejected_engine = {}, 0, 0
+    t0 = time.perf_counter()
+    for r in reqs:
+        now = time.perf_counter() - t0
+        if r.arrival > now:
+            time.sleep(r.arrival - now)
+        if max_queue and srv.stats()["queued"] >= max_queue:
+            rejected_full += 1
+            continue
+        wakes = g.request_wakes(r.scenario.meta)
+        counts = [w.n for w in wakes]
+        st, rid = srv.submit(counts, np.concatenate([w.pos for w in wakes]),
+                             np.concatenate([w.vor for w in wakes]), np.concatenate([w.rad for w in wakes]),
+                             np.concatenate([w.vol for w in wakes]), r.scenario.nu, r.scenario.dt,
+                             r.scenario.steps)
+        if st != 0:
+            rejected_engine += 1
+        else:
+            ids[rid] = r
+    t_arrivals = time.perf_counter() - t0
+    deadline = time.perf_counter() + drain
+    lat, done_inter = [], 0.0
+    pending = dict(ids)
+    while pending and time.perf_counter() < deadline:
+        for rid in list(pending):
+            if srv.poll(rid) in ("done", "rejected", "cancelled"):
+                out, ts, ta, td = srv.fetch(rid)
+                r = pending.pop(rid)
+                if out is not None:
+                    lat.append(td - ts)
+                    done_inter += 4.0 * r.scenario.meta["N"] ** 2 * r.scenario.steps
+        time.sleep(0.01)
+    elapsed = time.perf_counter() - t0
+    st = srv.stats()
+    srv.close()
+    lat.sort()
+    pct = (lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None)
+    return {"rate_per_s": rate, "arrival_window_s": duration, "arrivals": len(reqs),
+            "N_range": [n_lo, n_hi], "steps_range": [steps_lo, steps_hi],
+            "budget_bytes": budget, "max_step_interactions": cap, "max_active": max_active,
+            "max_queue": max_queue, "submitted": len(ids), "completed": len(lat),
+            "rejected": rejected_full + rejected_engine + int(st["rejected"]),
+            "queued_at_end": int(st["queued"]), "active_at_end": int(st["active"]),
+            "solves_per_s": len(lat) / elapsed, "p50_latency_s": pct(0.50), "p99_latency_s": pct(0.99),
+            "G_interactions_per_s_engine": st["interactions"] / max(1e-9, st["busy_seconds"]) / 1e9,
+            "elapsed_s": elapsed, "arrival_replay_s": t_arrivals}
+
+
 # --------------------------------------------------------------- GPU arm
 
 def run_pawan(args, rk: Ranks):
@@ -269,6 +389,7 @@ def run_pawan(args, rk: Ranks):
     prof = ctx.profile_read()
     ctx.profile(False)
     clk = clocks.stop()
+    clk["compute_processes"] = gpu_processes(gpu_index(rk.local))
     rk.barrier()
     ms_max = rk.max(ms)
     value = aggregate_rate(rk.world, 4.0 * N * N * args.steps, ms_max)
@@ -334,6 +455,19 @@ def run_pawan(args, rk: Ranks):
                        "h2d_bytes_per_step": int(hin.nbytes), "d2h_bytes_per_step": int(hout.nbytes),
                        "path": "pawan_system_set_states (pinned host) -> pawan_system_rk4 -> pawan_system_get_states"}
 
+        if rk.world == 1 and not args.no_suite:
+            line["batched"] = run_batch_leg(ctx)
+            # continuous batching at a capacity-matched load (request sizes scaled
+            # down so latencies are observable in seconds), against serving the
+            # same trace one request at a time
+            cm = dict(rate=120.0, duration=8.0, n_lo=1024, n_hi=16384, steps_lo=5, steps_hi=20,
+                      budget=120e9, cap=0.0, max_queue=0, drain=60.0)
+            line["served"] = {"capacity_matched": run_serving_leg(ctx, max_active=0, **cm),
+                              "capacity_matched_one_at_a_time": run_serving_leg(ctx, max_active=1, **cm),
+                              "specified_load": run_serving_leg(
+                                  ctx, rate=200.0, duration=10.0, n_lo=1024, n_hi=262144, steps_lo=50,
+                                  steps_hi=400, budget=120e9, cap=2e11, max_active=0, max_queue=64,
+                                  drain=0.0)}
         if rk.rank == 0 and rk.world == 1 and not args.no_cpu_baseline:
             try:
                 rate, n, tsec, threads = cpu_reference_sample(pos, vor, rad, vol, sc.nu, 10.0)

@@ -445,8 +445,11 @@ int system_alloc(pawan_system *sys) {
   std::vector<int> wid(n);
   for (size_t w = 0; w < sys->counts.size(); ++w)
     for (size_t i = 0; i < sys->counts[w]; ++i) wid[sys->offsets[w] + i] = (int)w;
-  PAWAN_CUDA(ctx, cudaMemcpy(sys->wake_id.p, wid.data(), n * sizeof(int), cudaMemcpyHostToDevice));
-  PAWAN_CUDA(ctx, cudaMemset(sys->X.p, 0, 6 * n * sizeof(double)));
+  // on the context's (non-blocking) stream, so later copies on it are ordered after these
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->wake_id.p, wid.data(), n * sizeof(int),
+                                  cudaMemcpyHostToDevice, ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemsetAsync(sys->X.p, 0, 6 * n * sizeof(double), ctx->stream));
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return PAWAN_OK;
 }
 

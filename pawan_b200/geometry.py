@@ -198,6 +198,16 @@ class Request:
     scenario: Scenario
 
 
+def request_wakes(meta: dict) -> List[Wake]:
+    """The wakes of a serving request from its drawn parameters (seeded)."""
+    sub = np.random.default_rng(meta["seed"])
+    n, R, sig, gam = meta["N"], meta["R"], meta["sigma"], meta["gamma"]
+    if meta["pair"]:
+        per = max(1, n // (2 * N_CORE))
+        return [ring(R, sig, gam, per, 0.0, sub), ring(R, sig, gam, per, R, sub)]
+    return [ring(R, sig, gam, max(1, n // N_CORE), 0.0, sub)]
+
+
 def serving_requests(rate: float = 200.0, duration: float = 60.0, seed: int = 5,
                      n_lo: int = 1024, n_hi: int = 262144, steps_lo: int = 50,
                      steps_hi: int = 400, dt: float = 0.005, build: bool = True) -> List[Request]:
@@ -217,15 +227,7 @@ def serving_requests(rate: float = 200.0, duration: float = 60.0, seed: int = 5,
         gam = rng.uniform(0.5, 2.0)
         nu = rng.uniform(0.0, 1e-3)
         meta = {"N": n, "pair": pair, "R": R, "sigma": sig, "gamma": gam, "seed": [seed, rid]}
-        if build:
-            sub = np.random.default_rng([seed, rid])
-            if pair:
-                per = max(1, n // (2 * N_CORE))
-                wakes = [ring(R, sig, gam, per, 0.0, sub), ring(R, sig, gam, per, R, sub)]
-            else:
-                wakes = [ring(R, sig, gam, n // N_CORE, 0.0, sub)]
-        else:
-            wakes = []
+        wakes = request_wakes(meta) if build else []
         out.append(Request(rid, t, Scenario(wakes, nu, dt, steps, name=f"req{rid}", meta=meta)))
         rid += 1
     return out
