@@ -143,6 +143,12 @@ int pawan_system_set_tiling(pawan_system *sys, const pawan_tiling *tiling);
 int pawan_system_get_tiling(pawan_system *sys, pawan_tiling *tiling);
 /* Times every compiled tiling on this system and keeps the fastest. */
 int pawan_system_autotune(pawan_system *sys);
+/* Device-side snapshot of the state (checkpoint) and its restore, for
+ * resuming a run or repeating steps from one state.  The reference's
+ * file-based save()/read() (src/wake/wake.cpp:58-85) is the on-disk
+ * counterpart; pawan_system_write_frame writes the .wake frames. */
+int pawan_system_checkpoint(pawan_system *sys);
+int pawan_system_restore(pawan_system *sys);
 /* Device address of the state [x | alpha] in union layout (6N doubles,
  * x = first 3N) for callers that keep data on the device. */
 int pawan_system_device_state(pawan_system *sys, double **state);

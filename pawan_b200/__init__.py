@@ -112,6 +112,8 @@ _SIGS = {
     "pawan_system_get_tiling": (ctypes.c_int, [_vp, ctypes.POINTER(Tiling)]),
     "pawan_system_autotune": (ctypes.c_int, [_vp]),
     "pawan_system_device_state": (ctypes.c_int, [_vp, ctypes.POINTER(_dp)]),
+    "pawan_system_checkpoint": (ctypes.c_int, [_vp]),
+    "pawan_system_restore": (ctypes.c_int, [_vp]),
     "pawan_batch_create": (ctypes.c_int, [_vp, ctypes.c_size_t, ctypes.POINTER(_vp), ctypes.POINTER(_vp)]),
     "pawan_batch_destroy": (None, [_vp]),
     "pawan_batch_rk4": (ctypes.c_int, [_vp, _dp, ctypes.c_double, ctypes.c_size_t, ctypes.c_int]),
@@ -383,6 +385,14 @@ class System:
     def autotune(self) -> dict:
         self.ctx.check(self._lib.pawan_system_autotune(self._h))
         return self.get_config()
+
+    def checkpoint(self):
+        """Device-side snapshot of the state."""
+        self.ctx.check(self._lib.pawan_system_checkpoint(self._h))
+
+    def restore(self):
+        """Back to the last checkpoint (device to device)."""
+        self.ctx.check(self._lib.pawan_system_restore(self._h))
 
 
 class Batch:

@@ -500,7 +500,7 @@ size_t pawan_system::device_bytes() const {
   return X.bytes() + Xs.bytes() + K1.bytes() + K2.bytes() + R.bytes() + rad.bytes() +
          vol.bytes() + wake_id.bytes() + pos32.bytes() + vor32.bytes() + poslo.bytes() +
          vorlo.bytes() + pos64.bytes() +
-         vor64.bytes() + diag_scratch.bytes() + diag_out.bytes() +
+         vor64.bytes() + diag_scratch.bytes() + diag_out.bytes() + Xc.bytes() +
          (plan ? plan->partial.bytes() : 0);
 }
 
@@ -951,6 +951,25 @@ int pawan_system_autotune(pawan_system *sys) {
   sys->ctx->tune_cache[std::make_tuple(sys->precision, sys->nu != 0.0 ? 1 : 0,
                                        (int)std::log2(std::max(1.0, n2)), 0)] = best;
   return system_ensure_plan(sys);
+}
+
+int pawan_system_checkpoint(pawan_system *sys) {
+  CHECK_SYS(sys);
+  pawan_ctx *ctx = sys->ctx;
+  if (!sys->has_particles) return fail(ctx, PAWAN_ERR_STATE, "particles not set");
+  if (!sys->Xc.p) PAWAN_CUDA(ctx, sys->Xc.alloc(6 * sys->n));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->Xc.p, sys->X.p, 6 * sys->n * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, ctx->stream));
+  return PAWAN_OK;
+}
+
+int pawan_system_restore(pawan_system *sys) {
+  CHECK_SYS(sys);
+  pawan_ctx *ctx = sys->ctx;
+  if (!sys->Xc.p) return fail(ctx, PAWAN_ERR_STATE, "no checkpoint taken");
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->X.p, sys->Xc.p, 6 * sys->n * sizeof(double),
+                                  cudaMemcpyDeviceToDevice, ctx->stream));
+  return pack_after_state(sys);
 }
 
 int pawan_system_device_state(pawan_system *sys, double **state) {

@@ -156,3 +156,15 @@ def test_wake_frames_match_reference_format(ctx):
     # headers (t, counts) identical; particle data within FP64 rounding
     assert np.array_equal(a[:3], b[:3])
     assert np.allclose(a, b, rtol=1e-12, atol=1e-15)
+
+
+def test_checkpoint_restore_repeats_a_step_bit_for_bit(ctx):
+    sc = g.ring_pair(n_stations=64, seed=44, nu=1e-3)
+    s = System.from_scenario(ctx, sc, "f32")
+    s.checkpoint()
+    s.rk4(sc.dt, 2)
+    a = s.get_states()
+    s.restore()
+    assert np.array_equal(s.get_states(), sc.state())
+    s.rk4(sc.dt, 2)
+    assert np.array_equal(s.get_states(), a)
