@@ -53,6 +53,8 @@ def parse():
                     help="main timed loop only (no autotune, FP64 comparison, e2e, CPU baseline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-suite", action="store_true", help="skip the batch and serving legs")
+    ap.add_argument("--configs", action="store_true",
+                    help="run every workload at its full length instead (minutes; one JSON line each)")
     return ap.parse_args()
 
 
@@ -492,8 +494,96 @@ def run_pawan(args, rk: Ranks):
         print(json.dumps(line), flush=True)
 
 
+def _finite_diag(d):
+    return {k: (v.tolist() if hasattr(v, "tolist") else v) for k, v in d.items()}
+
+
+def run_configs(args):
+    """Every workload at its specified length (one GPU; minutes)."""
+    import oracle
+    from pawan_b200 import Context, System, union_to_state
+    from pawan_b200 import geometry as g
+    ctx = Context(0)
+    emit = lambda d: print(json.dumps(d), flush=True)
+
+    # 1) single ring, N = 2,048, nu = 0, dt = 0.01, 200 steps: FP64 and FP32 on the
+    #    GPU, the reference's own __rk4 + __parallel on the CPU
+    sc = g.single_ring()
+    out = {"config": "single_ring", "N": sc.n, "steps": sc.steps, "dt": sc.dt}
+    for prec in ("f64_plain", "f32"):
+        s = System.from_scenario(ctx, sc, prec)
+        d0 = s.diagnose()
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        for k in range(sc.steps // 10):
+            s.rk4(sc.dt, 10)
+            if k == 9:
+                d100 = s.diagnose()
+        st = s.get_states()
+        t = time.perf_counter() - t0
+        out[prec] = {"seconds": t, "finite_at_end": bool(np.all(np.isfinite(st))),
+                     "diag_t0": _finite_diag(d0), "diag_step100": _finite_diag(d100),
+                     "G_interactions_per_s": 4.0 * sc.n ** 2 * sc.steps / t / 1e9}
+        s.close()
+    pos, vor, rad, vol = sc.union()
+    ref = oracle.RefSystem(sc.counts, pos, vor, rad, vol, sc.nu, parallel=True)
+    st = sc.state()
+    t0 = oracle.ref_wtime()
+    st = ref.rk4(st, sc.dt, sc.steps)
+    t = oracle.ref_wtime() - t0
+    out["cpu_reference"] = {"seconds": t, "threads": oracle.ref_max_threads(),
+                            "finite_at_end": bool(np.all(np.isfinite(st))),
+                            "G_interactions_per_s": 4.0 * sc.n ** 2 * sc.steps / t / 1e9,
+                            "path": "__rk4::step on __parallel (OpenMP), compiled from the reference sources"}
+    emit(out)
+
+    # 2) ring pair, N = 131,072, nu = 1e-4, dt = 0.005, 500 steps (FP32 pairs)
+    # 3) helical wake, N = 262,144, nu = 1e-3, dt = 0.002, 300 steps, FP64
+    #    diagnostics every 10 steps
+    for sc, every in ((g.ring_pair(), 50), (g.helical_wake(), 10)):
+        s = System.from_scenario(ctx, sc, "f32")
+        tile = s.autotune()
+        ctx.synchronize()
+        diags, t_diag = [], 0.0
+        ctx.profile(True)
+        t0 = time.perf_counter()
+        for k in range(sc.steps // every):
+            s.rk4(sc.dt, every)
+            td = time.perf_counter()
+            d = s.diagnose()
+            t_diag += time.perf_counter() - td
+            diags.append({"step": (k + 1) * every, "enstrophy": d["enstrophy"],
+                          "total_vorticity": d["total_vorticity"].tolist(),
+                          "linear_impulse": d["linear_impulse"].tolist()})
+        st = s.get_states()
+        t = time.perf_counter() - t0
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        emit({"config": sc.name, "N": sc.n, "steps": sc.steps, "dt": sc.dt, "nu": sc.nu, "tile": tile,
+              "seconds": t, "diagnostics_seconds": t_diag,
+              "G_interactions_per_s_incl_diagnostics": 4.0 * sc.n ** 2 * sc.steps / t / 1e9,
+              "pair_kernel_G_per_s": prof["pair_interactions"] / (prof["pair_ms"] * 1e-3) / 1e9,
+              "finite_at_end": bool(np.all(np.isfinite(st))), "diagnostics": diags[:3] + diags[-2:]})
+        s.close()
+
+    # 4) ragged batch, 512 solves x 100 steps
+    emit({"config": "ragged_batch", **run_batch_leg(ctx, steps=100)})
+
+    # 5) serving at the specified load (60 s of arrivals) and at a capacity-matched one
+    emit({"config": "serving_specified", **run_serving_leg(
+        ctx, rate=200.0, duration=60.0, n_lo=1024, n_hi=262144, steps_lo=50, steps_hi=400,
+        budget=120e9, cap=2e11, max_active=0, max_queue=64, drain=30.0)})
+    emit({"config": "serving_capacity_matched", **run_serving_leg(
+        ctx, rate=120.0, duration=30.0, n_lo=1024, n_hi=16384, steps_lo=5, steps_hi=20,
+        budget=120e9, cap=0.0, max_active=0, max_queue=0, drain=60.0)})
+    ctx.close()
+
+
 def main():
     args = parse()
+    if args.configs:
+        run_configs(args)
+        return
     rk = Ranks(args.gpus)
     try:
         if args.impl == "reference":
