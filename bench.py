@@ -549,6 +549,7 @@ def run_configs(args):
         t0 = time.perf_counter()
         for k in range(sc.steps // every):
             s.rk4(sc.dt, every)
+            ctx.synchronize()  # the steps run asynchronously; time the diagnostics alone
             td = time.perf_counter()
             d = s.diagnose()
             t_diag += time.perf_counter() - td
