@@ -59,39 +59,43 @@ struct NoallocScratch {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoallocScratch)];
 
 // Pack: positions relative to particle 0 as FP32 hi/lo, strengths hi/lo,
-// s^2/2 and volume; the bounding box of each 128-particle tile; per-block
-// maxima of the smoothing radius and of the distance from particle 0.
+// s^2/2 and volume; the bounding box (with the range of s^2/2 in w) of each
+// 128-particle tile; per-block maxima of the smoothing radius and of the
+// distance from particle 0.
 __global__ void __launch_bounds__(kStageThreads)
     noalloc_prepare(NoallocScratch *S, const double *pos, const double *vor, const double *rad,
                     const double *vol, int n) {
-  __shared__ float lo[3][kStageThreads], hi[3][kStageThreads];
+  __shared__ float lo[4][kStageThreads], hi[4][kStageThreads];
   __shared__ float ms[kStageThreads], me[kStageThreads];
   const int t = threadIdx.x;
   const int l = blockIdx.x * kStageThreads + t;
   const bool has = l < n;
-  float3 p = make_float3(0.f, 0.f, 0.f);
+  float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
   float s_l = 0.f, e2 = 0.f;
   if (has) {
     const double rx = pos[3 * l] - pos[0], ry = pos[3 * l + 1] - pos[1], rz = pos[3 * l + 2] - pos[2];
     const float hx = (float)rx, hy = (float)ry, hz = (float)rz;
     const double s = rad[l];
     const float ax = (float)vor[3 * l], ay = (float)vor[3 * l + 1], az = (float)vor[3 * l + 2];
-    S->pos32[l] = make_float4(hx, hy, hz, (float)(0.5 * s * s));
+    const float hw = (float)(0.5 * s * s);
+    S->pos32[l] = make_float4(hx, hy, hz, hw);
     S->poslo[l] = make_float4((float)(rx - (double)hx), (float)(ry - (double)hy),
                               (float)(rz - (double)hz), 0.f);
     S->vor32[l] = make_float4(ax, ay, az, (float)vol[l]);
     S->vorlo[l] = make_float4((float)(vor[3 * l] - (double)ax), (float)(vor[3 * l + 1] - (double)ay),
                               (float)(vor[3 * l + 2] - (double)az), 0.f);
-    p = make_float3(hx, hy, hz);
+    p = make_float4(hx, hy, hz, hw);
     s_l = (float)s;
     e2 = (float)(rx * rx + ry * ry + rz * rz);
   }
   lo[0][t] = has ? p.x : INFINITY;
   lo[1][t] = has ? p.y : INFINITY;
   lo[2][t] = has ? p.z : INFINITY;
+  lo[3][t] = has ? p.w : INFINITY;
   hi[0][t] = has ? p.x : -INFINITY;
   hi[1][t] = has ? p.y : -INFINITY;
   hi[2][t] = has ? p.z : -INFINITY;
+  hi[3][t] = has ? p.w : -INFINITY;
   ms[t] = s_l;
   me[t] = e2;
   __syncthreads();
@@ -102,7 +106,7 @@ __global__ void __launch_bounds__(kStageThreads)
     }
     if ((t % kNaTB) < s && s < kNaTB) {
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
+      for (int k = 0; k < 4; ++k) {
         lo[k][t] = fminf(lo[k][t], lo[k][t + s]);
         hi[k][t] = fmaxf(hi[k][t], hi[k][t + s]);
       }
@@ -111,8 +115,8 @@ __global__ void __launch_bounds__(kStageThreads)
   }
   if ((t % kNaTB) == 0 && l < n) {
     const int b = l / kNaTB;
-    S->boxes[2 * b] = make_float4(lo[0][t], lo[1][t], lo[2][t], 0.f);
-    S->boxes[2 * b + 1] = make_float4(hi[0][t], hi[1][t], hi[2][t], 0.f);
+    S->boxes[2 * b] = make_float4(lo[0][t], lo[1][t], lo[2][t], lo[3][t]);
+    S->boxes[2 * b + 1] = make_float4(hi[0][t], hi[1][t], hi[2][t], hi[3][t]);
   }
   if (t == 0) {
     S->block_max[2 * blockIdx.x] = ms[0];

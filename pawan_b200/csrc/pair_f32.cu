@@ -32,18 +32,32 @@
 //    (accurate for nearly parallel and antiparallel strengths alike), and
 //    diffusion as v_i delta + (v_i - v_j) alpha_i (= v_i alpha_j - v_j alpha_i).
 //    ~94 FP32 instructions per pair.
-//  * far tiles: hi positions only, and the per-target sums
-//      U = sum qh (alpha_j x d), Q = sum qh alpha_j, G = sum fh [alpha_i.(alpha_j x d)] d,
+//  * far tiles: hi positions relative to the centre c of the source tile's
+//    box, x' = x - c, and two crosses formed once per particle and tile
+//    instead of once per pair, beta_j = alpha_j x x'_j (when the tile is
+//    staged) and gamma_i = x'_i x alpha_i (per target), so that
+//      alpha_j x d = alpha_j x x'_i - beta_j,
+//      alpha_i.(alpha_j x d) = alpha_j.gamma_i - alpha_i.beta_j.
+//    Per target the sums
+//      W = sum qh beta_j, Q = sum qh alpha_j, G = sum fh [alpha_i.(alpha_j x d)] d,
 //      E = sum Dp alpha_j, V = sum Dp v_j
-//    from which dalpha = alpha_i x (A Q) + 3A G + 15 nu A (v_i E - V alpha_i):
-//    49 FP32 instructions per pair (45 without diffusion).
+//    give u = A (Q x x'_i - W) and
+//    dalpha = alpha_i x (A Q) + 3A G + 15 nu A (v_i E - V alpha_i).
+//    The split costs accuracy where |x'| >> |d|; a tile pair is far only when
+//    its box gap is at least the source box's half-diagonal, which bounds
+//    |x'_i| + |x'_j| by 3 |d|.  When both tiles hold one smoothing radius
+//    (sigma^2 = 2h for every pair) the factor sigma^2 and the constants leave
+//    the pair loop for the per-tile fold (kernel_scalars_uniform).
+//    39 FP32 instructions per pair with one radius (43 with several; 4 fewer
+//    without diffusion).
 // After each tile both are folded into six FP64 sums (u, dalpha) with the
 // target's strength in FP64 (hi + lo).
 //
 // Layout: one persistent block per SM slot takes work items (target tile x
 // source chunk) from a counter; sources stream through a two-stage shared-memory
-// ring, each thread loading one source (four float4) for the next tile while
-// the block computes the current one.  The result of an item (u, dalpha in
+// ring, each thread starting asynchronous copies (cp.async, no registers held)
+// of one source (four float4) for the next tile while the block computes the
+// current one.  The result of an item (u, dalpha in
 // FP64) goes to its chunk of the partial buffer, which the stage kernel
 // reduces in chunk order.
 #include "device.cuh"
@@ -53,35 +67,58 @@ namespace pawan {
 namespace {
 
 struct Acc32 {
-  float ux, uy, uz;
+  float ux, uy, uz;  // far: sum qh beta_j         near: sum qh (alpha_j x d)
   float qx, qy, qz;  // far: sum qh alpha_j        near: sum qh (alpha_i x delta)
   float gx, gy, gz;
   float ex, ey, ez;  // far: sum Dp alpha_j        near: sum Dp delta
   float ev;          // far: sum Dp v_j            near: sum Dp (v_i - v_j)
 };
 
+// A target's hi parts (registers for the whole work item); the lo parts are
+// read from global memory only for near tiles.
 struct Target {
   float xh, yh, zh, h;
-  float xl, yl, zl;
   float ah, bh, ch, v;  // strength hi (x, y, z) and volume
-  float al, bl, cl;     // strength lo
 };
 
-// A source that contributes exactly zero: far away (every kernel factor
-// underflows to 0 and stays finite) with zero strength and volume.
-__device__ __forceinline__ void load_source(const SegDesc &sg, int j, int s1, float4 (&r)[4]) {
-  if (j < s1) {
-    r[0] = __ldg(sg.pos32 + j);
-    r[1] = __ldg(sg.vor32 + j);
-    r[2] = __ldg(sg.poslo + j);
-    r[3] = __ldg(sg.vorlo + j);
-  } else {
-    r[0] = make_float4(1e18f, 1e18f, 1e18f, 1.0f);
-    r[1] = make_float4(0.f, 0.f, 0.f, 0.f);
-    r[2] = make_float4(0.f, 0.f, 0.f, 0.f);
-    r[3] = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
+// A target relative to the current far source tile.
+struct FarTarget {
+  float x, y, z;     // x'_i = x_i - c
+  float gx, gy, gz;  // gamma_i = x'_i x alpha_i
+};
+
+__device__ __forceinline__ float rcp_approx(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
 }
+
+__device__ __forceinline__ void cp_async16(float4 *smem, const float4 *gmem) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
+}
+
+// Starts the copy of source j into one shared-memory slot (pos32, vor32,
+// poslo, vorlo), or writes a source that contributes exactly zero when j is
+// past the chunk: far away (every kernel factor underflows to 0 and stays
+// finite) with zero strength and volume.
+__device__ __forceinline__ void stage_source(const SegDesc &sg, int j, int s1, float4 *p,
+                                             float4 *v, float4 *pl, float4 *vl) {
+  if (j < s1) {
+    cp_async16(p, sg.pos32 + j);
+    cp_async16(v, sg.vor32 + j);
+    cp_async16(pl, sg.poslo + j);
+    cp_async16(vl, sg.vorlo + j);
+  } else {
+    *p = make_float4(1e18f, 1e18f, 1e18f, 1.0f);
+    *v = make_float4(0.f, 0.f, 0.f, 0.f);
+    *pl = make_float4(0.f, 0.f, 0.f, 0.f);
+    *vl = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+__device__ __forceinline__ void wait_staged() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 // q, F and the diffusion factor of one pair in units of A = 1/(4 pi), from
 // sigma^2, w = (rho^2 + sigma^2)^-1/2 and ri = 1/rho (u = sigma^2 w^2):
@@ -104,32 +141,66 @@ __device__ __forceinline__ void kernel_scalars(float sig2, float w, float ri, fl
   fh = fmaf(2.5f, zc, -qh) * ri2;
 }
 
-template <bool DIFF, int P, int R, int NSRC, int U>
-__device__ __forceinline__ void tile_far(const float4 *__restrict__ sp,
-                                         const float4 *__restrict__ sv, int g,
-                                         const Target (&T)[R], Acc32 (&a)[R]) {
+// kernel_scalars for sigma^2 = 2h the same for every pair of the tile, with
+// the factors that do not vary per pair left to the per-tile fold: returns
+//   qs = qh / sigma^2,  fs = fh / sigma^2,  ds = Dp / 32,
+// from u' = h w^2 = u/2 and v' = u' w = v/2 (so ds = v'^5):
+//   ph = (1 + u') w^2 / rho,  qs = (ph - 240 sigma^2 ds) / rho^2,
+//   fs = (80 ds - qs) / rho^2.
+// 1/rho^2 comes from the MUFU reciprocal; 12 FP32 instructions.
+__device__ __forceinline__ void kernel_scalars_uniform(float h, float c240, float w, float ri,
+                                                       float r2, float &qs, float &fs, float &ds) {
+  const float y = w * w;
+  const float u = h * y;
+  const float v = u * w;
+  const float v2 = v * v;
+  ds = v2 * v2 * v;
+  const float ph = fmaf(u, y, y) * ri;
+  const float ri2 = rcp_approx(r2);
+  qs = fmaf(c240, ds, ph) * ri2;
+  fs = fmaf(80.f, ds, -qs) * ri2;
+}
+
+// Far tile, shared-memory format (written when the tile is staged):
+//   sa[j] = (x'_j, h_j),  sb[j] = (alpha_j, v_j),  sc[j] = (beta_j, 0).
+// UNI: every pair has sigma^2 = 2 hu (sums in the units of
+// kernel_scalars_uniform).
+template <bool DIFF, bool UNI, int P, int R, int NSRC, int U>
+__device__ __forceinline__ void tile_far(const float4 *__restrict__ sa,
+                                         const float4 *__restrict__ sb,
+                                         const float4 *__restrict__ sc, int g,
+                                         const Target (&T)[R], const FarTarget (&F)[R], float hu,
+                                         Acc32 (&a)[R]) {
+  const float s2u = 2.f * hu;
+  const float c240 = -480.f * hu;
 #pragma unroll U
   for (int k = 0; k < NSRC / P; ++k) {
     const int jj = g + P * k;
-    const float4 p = sp[jj];
-    const float4 s = sv[jj];
+    const float4 p = sa[jj];
+    const float4 s = sb[jj];
+    const float4 b = sc[jj];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const float dx = T[r].xh - p.x, dy = T[r].yh - p.y, dz = T[r].zh - p.z;
+      const float dx = F[r].x - p.x, dy = F[r].y - p.y, dz = F[r].z - p.z;
       const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-      const float sig2 = T[r].h + p.w;
-      const float w = rsqrtf(r2 + sig2);
-      const float ri = rsqrtf(r2);
       float qh, fh, dp;
-      kernel_scalars(sig2, w, ri, qh, fh, dp);
-      const float cx = fmaf(s.y, dz, -s.z * dy);
-      const float cy = fmaf(s.z, dx, -s.x * dz);
-      const float cz = fmaf(s.x, dy, -s.y * dx);
-      const float t = fmaf(T[r].ch, cz, fmaf(T[r].bh, cy, T[r].ah * cx));
+      if (UNI) {
+        const float w = rsqrtf(r2 + s2u);
+        const float ri = rsqrtf(r2);
+        kernel_scalars_uniform(hu, c240, w, ri, r2, qh, fh, dp);
+      } else {
+        const float sig2 = T[r].h + p.w;
+        const float w = rsqrtf(r2 + sig2);
+        const float ri = rsqrtf(r2);
+        kernel_scalars(sig2, w, ri, qh, fh, dp);
+      }
+      // alpha_i.(alpha_j x d) = alpha_j.gamma_i - alpha_i.beta_j
+      const float t = fmaf(-T[r].ch, b.z, fmaf(-T[r].bh, b.y, fmaf(-T[r].ah, b.x,
+                      fmaf(s.z, F[r].gz, fmaf(s.y, F[r].gy, s.x * F[r].gx)))));
       const float ft = fh * t;
-      a[r].ux = fmaf(qh, cx, a[r].ux);
-      a[r].uy = fmaf(qh, cy, a[r].uy);
-      a[r].uz = fmaf(qh, cz, a[r].uz);
+      a[r].ux = fmaf(qh, b.x, a[r].ux);
+      a[r].uy = fmaf(qh, b.y, a[r].uy);
+      a[r].uz = fmaf(qh, b.z, a[r].uz);
       a[r].qx = fmaf(qh, s.x, a[r].qx);
       a[r].qy = fmaf(qh, s.y, a[r].qy);
       a[r].qz = fmaf(qh, s.z, a[r].qz);
@@ -246,12 +317,15 @@ __device__ __forceinline__ void cross_accurate(float ax, float ay, float az, flo
   wz = det2(ax, ay, bx, by) + fmaf(ax, my, fmaf(-ay, mx, fmaf(lx, by, -ly * bx)));
 }
 
+// Near tile, shared-memory format: sp, sv, spl, svl = pos32, vor32, poslo,
+// vorlo of the sources; tpl, tvl = poslo, vorlo of the targets.
 template <bool DIFF, bool CHECK, int P, int R, int NSRC>
 __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
                                           const float4 *__restrict__ sv,
                                           const float4 *__restrict__ spl,
                                           const float4 *__restrict__ svl, int g,
                                           const int (&skip)[R], const Target (&T)[R],
+                                          const float4 (&tpl)[R], const float4 (&tvl)[R],
                                           Acc32 (&a)[R]) {
   // near tiles are a few percent of the work: no unrolling keeps the register
   // budget of the far loop
@@ -264,9 +338,9 @@ __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
     const float4 sl = svl[jj];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const float dx = (T[r].xh - p.x) + (T[r].xl - pl.x);
-      const float dy = (T[r].yh - p.y) + (T[r].yl - pl.y);
-      const float dz = (T[r].zh - p.z) + (T[r].zl - pl.z);
+      const float dx = (T[r].xh - p.x) + (tpl[r].x - pl.x);
+      const float dy = (T[r].yh - p.y) + (tpl[r].y - pl.y);
+      const float dz = (T[r].zh - p.z) + (tpl[r].z - pl.z);
       const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
       const float sig2 = T[r].h + p.w;
       const float w = rsqrtf(r2 + sig2);
@@ -279,8 +353,8 @@ __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
       const float cz = fmaf(s.x, dy, -s.y * dx);
       // stretching: alpha_i x alpha_j from the hi/lo strengths
       float wx, wy, wz;
-      cross_accurate(T[r].ah, T[r].bh, T[r].ch, T[r].al, T[r].bl, T[r].cl, s.x, s.y, s.z, sl.x, sl.y,
-                     sl.z, wx, wy, wz);
+      cross_accurate(T[r].ah, T[r].bh, T[r].ch, tvl[r].x, tvl[r].y, tvl[r].z, s.x, s.y, s.z, sl.x,
+                     sl.y, sl.z, wx, wy, wz);
       const float t = fmaf(dz, wz, fmaf(dy, wy, dx * wx));
       float ft = fh * t;
       if (CHECK) {
@@ -300,9 +374,9 @@ __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
       a[r].gz = fmaf(ft, dz, a[r].gz);
       if (DIFF) {
         // delta = alpha_j - alpha_i from the hi/lo strengths
-        const float ex = (s.x - T[r].ah) + (sl.x - T[r].al);
-        const float ey = (s.y - T[r].bh) + (sl.y - T[r].bl);
-        const float ez = (s.z - T[r].ch) + (sl.z - T[r].cl);
+        const float ex = (s.x - T[r].ah) + (sl.x - tvl[r].x);
+        const float ey = (s.y - T[r].bh) + (sl.y - tvl[r].y);
+        const float ez = (s.z - T[r].ch) + (sl.z - tvl[r].z);
         a[r].ex = fmaf(dp, ex, a[r].ex);
         a[r].ey = fmaf(dp, ey, a[r].ey);
         a[r].ez = fmaf(dp, ez, a[r].ez);
@@ -317,6 +391,16 @@ __device__ __forceinline__ float box_gap2(float4 alo, float4 ahi, float4 blo, fl
   const float gy = fmaxf(0.f, fmaxf(alo.y - bhi.y, blo.y - ahi.y));
   const float gz = fmaxf(0.f, fmaxf(alo.z - bhi.z, blo.z - ahi.z));
   return gx * gx + gy * gy + gz * gz;
+}
+
+// Far formulation allowed: box gap positive and at least max(near radius,
+// half-diagonal of the source box).
+__device__ __forceinline__ bool far_tiles(float4 tlo, float4 thi, float4 slo, float4 shi,
+                                          float near2) {
+  const float ex = shi.x - slo.x, ey = shi.y - slo.y, ez = shi.z - slo.z;
+  const float half_diag2 = 0.25f * (ex * ex + ey * ey + ez * ez);
+  const float gap2 = box_gap2(tlo, thi, slo, shi);
+  return gap2 > 0.f && gap2 >= near2 && gap2 >= half_diag2;
 }
 
 // Threads per target P > 1 split a tile's sources (R = 1); targets per thread
@@ -355,28 +439,21 @@ __global__ void __launch_bounds__(TB, MINB)
     int ti[R];
     bool valid[R];
     Target T[R];
-    double ax[R], ay[R], az[R];
+    float al[R], bl[R], cl[R];  // strength lo: the folds use alpha_i = hi + lo in FP64
     double ou[R][3], oa[R][3];
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       ti[r] = w.t0 + lt + r * TG;
       valid[r] = ti[r] < sg.n;
-      float4 a = make_float4(0.f, 0.f, 0.f, 1.f), b = make_float4(0.f, 0.f, 0.f, 0.f);
-      float4 c = b, d = b;
+      float4 a = make_float4(0.f, 0.f, 0.f, 1.f), b = make_float4(0.f, 0.f, 0.f, 0.f), d = b;
       if (valid[r]) {
         a = __ldg(sg.pos32 + ti[r]);
         b = __ldg(sg.vor32 + ti[r]);
-        c = __ldg(sg.poslo + ti[r]);
         d = __ldg(sg.vorlo + ti[r]);
       }
       T[r].xh = a.x; T[r].yh = a.y; T[r].zh = a.z; T[r].h = a.w;
       T[r].ah = b.x; T[r].bh = b.y; T[r].ch = b.z; T[r].v = b.w;
-      T[r].xl = c.x; T[r].yl = c.y; T[r].zl = c.z;
-      T[r].al = d.x; T[r].bl = d.y; T[r].cl = d.z;
-      // target strength in FP64 (hi + lo) for the per-tile folds
-      ax[r] = (double)T[r].ah + (double)T[r].al;
-      ay[r] = (double)T[r].bh + (double)T[r].bl;
-      az[r] = (double)T[r].ch + (double)T[r].cl;
+      al[r] = d.x; bl[r] = d.y; cl[r] = d.z;
 #pragma unroll
       for (int k = 0; k < 3; ++k) ou[r][k] = oa[r][k] = 0.0;
     }
@@ -392,7 +469,8 @@ __global__ void __launch_bounds__(TB, MINB)
       T2.c = bc2(T[0].ch);
     }
 
-    // box of the target tile: union of the source-tile boxes it covers
+    // box of the target tile: union of the source-tile boxes it covers (w:
+    // range of h)
     float4 tlo = __ldg(sg.boxes + 2 * (w.t0 / TB));
     float4 thi = __ldg(sg.boxes + 2 * (w.t0 / TB) + 1);
 #pragma unroll
@@ -400,90 +478,142 @@ __global__ void __launch_bounds__(TB, MINB)
       if (w.t0 + q * TB < sg.n) {
         const float4 l2 = __ldg(sg.boxes + 2 * (w.t0 / TB + q));
         const float4 h2 = __ldg(sg.boxes + 2 * (w.t0 / TB + q) + 1);
-        tlo = make_float4(fminf(tlo.x, l2.x), fminf(tlo.y, l2.y), fminf(tlo.z, l2.z), 0.f);
-        thi = make_float4(fmaxf(thi.x, h2.x), fmaxf(thi.y, h2.y), fmaxf(thi.z, h2.z), 0.f);
+        tlo = make_float4(fminf(tlo.x, l2.x), fminf(tlo.y, l2.y), fminf(tlo.z, l2.z),
+                          fminf(tlo.w, l2.w));
+        thi = make_float4(fmaxf(thi.x, h2.x), fmaxf(thi.y, h2.y), fmaxf(thi.z, h2.z),
+                          fmaxf(thi.w, h2.w));
       }
     }
 
     const int ntiles = (w.s1 - w.s0 + TB - 1) / TB;
-    float4 rs[4];
-    load_source(sg, w.s0 + tid, w.s1, rs);
+    stage_source(sg, w.s0 + tid, w.s1, &sp[0][tid], &sv[0][tid], &spl[0][tid], &svl[0][tid]);
     for (int t = 0; t < ntiles; ++t) {
       const int buf = t & 1;
-      sp[buf][tid] = rs[0];
-      sv[buf][tid] = rs[1];
-      spl[buf][tid] = rs[2];
-      svl[buf][tid] = rs[3];
+      const int ts = w.s0 + t * TB;
+      const float4 slo = __ldg(sg.boxes + 2 * (ts / TB));
+      const float4 shi = __ldg(sg.boxes + 2 * (ts / TB) + 1);
+      const bool diag = (ts < w.t0 + TPB) && (w.t0 < ts + TB);
+      const bool near = diag || !far_tiles(tlo, thi, slo, shi, sg.near2);
+      // one smoothing radius over both tiles
+      const bool uni = tlo.w == thi.w && slo.w == shi.w && tlo.w == slo.w;
+      const float cx = 0.5f * (slo.x + shi.x), cy = 0.5f * (slo.y + shi.y),
+                  cz = 0.5f * (slo.z + shi.z);
+      // this thread's own slot of the tile: wait for its copies, then rewrite
+      // it in the far format (or the packed one); the barrier publishes the
+      // tile and retires the previous one, whose buffer the next copies reuse
+      wait_staged();
       if (PK) {
+        const float4 p0 = sp[buf][tid], p1 = sv[buf][tid];
         const int k = tid >> 1, hf = tid & 1;
         float *q0 = reinterpret_cast<float *>(&fq[0][buf][k]);
         float *q1 = reinterpret_cast<float *>(&fq[1][buf][k]);
         float *q2 = reinterpret_cast<float *>(&fq[2][buf][k]);
         float *q3 = reinterpret_cast<float *>(&fq[3][buf][k]);
-        q0[hf] = -rs[0].x;
-        q0[2 + hf] = -rs[0].y;
-        q1[hf] = -rs[0].z;
-        q1[2 + hf] = rs[0].w;
-        q2[hf] = rs[1].x;
-        q2[2 + hf] = rs[1].y;
-        q3[hf] = rs[1].z;
-        q3[2 + hf] = rs[1].w;
+        q0[hf] = -p0.x;
+        q0[2 + hf] = -p0.y;
+        q1[hf] = -p0.z;
+        q1[2 + hf] = p0.w;
+        q2[hf] = p1.x;
+        q2[2 + hf] = p1.y;
+        q3[hf] = p1.z;
+        q3[2 + hf] = p1.w;
+      } else if (!near) {
+        const float4 p0 = sp[buf][tid], p1 = sv[buf][tid];
+        const float px = p0.x - cx, py = p0.y - cy, pz = p0.z - cz;
+        sp[buf][tid] = make_float4(px, py, pz, p0.w);
+        spl[buf][tid] = make_float4(fmaf(p1.y, pz, -p1.z * py), fmaf(p1.z, px, -p1.x * pz),
+                                    fmaf(p1.x, py, -p1.y * px), 0.f);
       }
       __syncthreads();
-      const int ts = w.s0 + t * TB;
-      if (t + 1 < ntiles) load_source(sg, ts + TB + tid, w.s1, rs);
+      if (t + 1 < ntiles)
+        stage_source(sg, ts + TB + tid, w.s1, &sp[buf ^ 1][tid], &sv[buf ^ 1][tid],
+                     &spl[buf ^ 1][tid], &svl[buf ^ 1][tid]);
       Acc32 a[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) a[r] = Acc32{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-      const bool diag = (ts < w.t0 + TPB) && (w.t0 < ts + TB);
-      const float4 slo = __ldg(sg.boxes + 2 * (ts / TB));
-      const float4 shi = __ldg(sg.boxes + 2 * (ts / TB) + 1);
-      const bool near = diag || box_gap2(tlo, thi, slo, shi) < sg.near2;
-      if (!near) {
-        if (PK) {
-          Acc2 b;
-          b.ux = b.uy = b.uz = b.qx = b.qy = b.qz = b.gx = b.gy = b.gz = make_float2(0.f, 0.f);
-          b.ex = b.ey = b.ez = b.ev = make_float2(0.f, 0.f);
-          tile_far_packed<DIFF, TB, U>(fq[0][buf], fq[1][buf], fq[2][buf], fq[3][buf], T2, b);
-          a[0].ux = -(b.ux.x + b.ux.y);
-          a[0].uy = -(b.uy.x + b.uy.y);
-          a[0].uz = -(b.uz.x + b.uz.y);
-          a[0].qx = -(b.qx.x + b.qx.y);
-          a[0].qy = -(b.qy.x + b.qy.y);
-          a[0].qz = -(b.qz.x + b.qz.y);
-          a[0].gx = b.gx.x + b.gx.y;
-          a[0].gy = b.gy.x + b.gy.y;
-          a[0].gz = b.gz.x + b.gz.y;
-          a[0].ex = b.ex.x + b.ex.y;
-          a[0].ey = b.ey.x + b.ey.y;
-          a[0].ez = b.ez.x + b.ez.y;
-          a[0].ev = b.ev.x + b.ev.y;
-        } else {
-          tile_far<DIFF, P, R, TB, U>(sp[buf], sv[buf], g, T, a);
+      double ax[R], ay[R], az[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        ax[r] = (double)T[r].ah + (double)al[r];
+        ay[r] = (double)T[r].bh + (double)bl[r];
+        az[r] = (double)T[r].ch + (double)cl[r];
+      }
+      if (!near && PK) {
+        Acc2 b;
+        b.ux = b.uy = b.uz = b.qx = b.qy = b.qz = b.gx = b.gy = b.gz = make_float2(0.f, 0.f);
+        b.ex = b.ey = b.ez = b.ev = make_float2(0.f, 0.f);
+        tile_far_packed<DIFF, TB, U>(fq[0][buf], fq[1][buf], fq[2][buf], fq[3][buf], T2, b);
+        const double Qx = -A * (b.qx.x + b.qx.y), Qy = -A * (b.qy.x + b.qy.y),
+                     Qz = -A * (b.qz.x + b.qz.y);
+        ou[0][0] -= A * (b.ux.x + b.ux.y);
+        ou[0][1] -= A * (b.uy.x + b.uy.y);
+        ou[0][2] -= A * (b.uz.x + b.uz.y);
+        oa[0][0] += (ay[0] * Qz - az[0] * Qy) + 3.0 * A * (b.gx.x + b.gx.y);
+        oa[0][1] += (az[0] * Qx - ax[0] * Qz) + 3.0 * A * (b.gy.x + b.gy.y);
+        oa[0][2] += (ax[0] * Qy - ay[0] * Qx) + 3.0 * A * (b.gz.x + b.gz.y);
+        if (DIFF) {
+          const double v = T[0].v, ev = b.ev.x + b.ev.y;
+          oa[0][0] += cnu * (v * (b.ex.x + b.ex.y) - ev * ax[0]);
+          oa[0][1] += cnu * (v * (b.ey.x + b.ey.y) - ev * ay[0]);
+          oa[0][2] += cnu * (v * (b.ez.x + b.ez.y) - ev * az[0]);
         }
+      } else if (!near) {
+        FarTarget F[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-          const double Qx = A * a[r].qx, Qy = A * a[r].qy, Qz = A * a[r].qz;
-          oa[r][0] += (ay[r] * Qz - az[r] * Qy) + 3.0 * A * a[r].gx;
-          oa[r][1] += (az[r] * Qx - ax[r] * Qz) + 3.0 * A * a[r].gy;
-          oa[r][2] += (ax[r] * Qy - ay[r] * Qx) + 3.0 * A * a[r].gz;
+          F[r].x = T[r].xh - cx;
+          F[r].y = T[r].yh - cy;
+          F[r].z = T[r].zh - cz;
+          F[r].gx = fmaf(F[r].y, T[r].ch, -F[r].z * T[r].bh);
+          F[r].gy = fmaf(F[r].z, T[r].ah, -F[r].x * T[r].ch);
+          F[r].gz = fmaf(F[r].x, T[r].bh, -F[r].y * T[r].ah);
+        }
+        if (uni)
+          tile_far<DIFF, true, P, R, TB, U>(sp[buf], sv[buf], spl[buf], g, T, F, slo.w, a);
+        else
+          tile_far<DIFF, false, P, R, TB, U>(sp[buf], sv[buf], spl[buf], g, T, F, 0.f, a);
+        // undo the uniform-radius scaling: qh = sigma^2 qs, fh = sigma^2 fs, Dp = 32 ds
+        const double s2 = uni ? 2.0 * (double)slo.w : 1.0;
+        const double As2 = A * s2;
+        const double cd = uni ? 32.0 * cnu : cnu;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const double Qx = As2 * a[r].qx, Qy = As2 * a[r].qy, Qz = As2 * a[r].qz;
+          const double xp = F[r].x, yp = F[r].y, zp = F[r].z;
+          // u = A sigma^2 (Q x x' - W)
+          ou[r][0] += (Qy * zp - Qz * yp) - As2 * a[r].ux;
+          ou[r][1] += (Qz * xp - Qx * zp) - As2 * a[r].uy;
+          ou[r][2] += (Qx * yp - Qy * xp) - As2 * a[r].uz;
+          oa[r][0] += (ay[r] * Qz - az[r] * Qy) + 3.0 * As2 * a[r].gx;
+          oa[r][1] += (az[r] * Qx - ax[r] * Qz) + 3.0 * As2 * a[r].gy;
+          oa[r][2] += (ax[r] * Qy - ay[r] * Qx) + 3.0 * As2 * a[r].gz;
           if (DIFF) {
             const double v = T[r].v;
-            oa[r][0] += cnu * (v * a[r].ex - (double)a[r].ev * ax[r]);
-            oa[r][1] += cnu * (v * a[r].ey - (double)a[r].ev * ay[r]);
-            oa[r][2] += cnu * (v * a[r].ez - (double)a[r].ev * az[r]);
+            oa[r][0] += cd * (v * a[r].ex - (double)a[r].ev * ax[r]);
+            oa[r][1] += cd * (v * a[r].ey - (double)a[r].ev * ay[r]);
+            oa[r][2] += cd * (v * a[r].ez - (double)a[r].ev * az[r]);
           }
         }
       } else {
         int skip[R];
-#pragma unroll
-        for (int r = 0; r < R; ++r) skip[r] = ti[r] - ts;
-        if (diag)
-          tile_near<DIFF, true, P, R, TB>(sp[buf], sv[buf], spl[buf], svl[buf], g, skip, T, a);
-        else
-          tile_near<DIFF, false, P, R, TB>(sp[buf], sv[buf], spl[buf], svl[buf], g, skip, T, a);
+        float4 tpl[R], tvl[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
+          skip[r] = ti[r] - ts;
+          tpl[r] = valid[r] ? __ldg(sg.poslo + ti[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
+          tvl[r] = valid[r] ? __ldg(sg.vorlo + ti[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        if (diag)
+          tile_near<DIFF, true, P, R, TB>(sp[buf], sv[buf], spl[buf], svl[buf], g, skip, T, tpl,
+                                          tvl, a);
+        else
+          tile_near<DIFF, false, P, R, TB>(sp[buf], sv[buf], spl[buf], svl[buf], g, skip, T, tpl,
+                                           tvl, a);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          ou[r][0] += A * a[r].ux;
+          ou[r][1] += A * a[r].uy;
+          ou[r][2] += A * a[r].uz;
           oa[r][0] += A * a[r].qx + 3.0 * A * a[r].gx;
           oa[r][1] += A * a[r].qy + 3.0 * A * a[r].gy;
           oa[r][2] += A * a[r].qz + 3.0 * A * a[r].gz;
@@ -494,12 +624,6 @@ __global__ void __launch_bounds__(TB, MINB)
             oa[r][2] += cnu * (v * a[r].ez + (double)a[r].ev * az[r]);
           }
         }
-      }
-#pragma unroll
-      for (int r = 0; r < R; ++r) {
-        ou[r][0] += A * a[r].ux;
-        ou[r][1] += A * a[r].uy;
-        ou[r][2] += A * a[r].uz;
       }
     }
 

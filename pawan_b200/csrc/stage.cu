@@ -20,14 +20,15 @@ namespace {
 
 // Packs one particle: FP32 hi/lo pairs of the position relative to the
 // system's origin and of the strength, plus the FP64 copies.  Returns the hi
-// position for the tile's bounding box.
-__device__ __forceinline__ float3 pack(const StageDesc &d, int l, const double x[6]) {
+// position and h = s^2/2 for the tile's bounding box.
+__device__ __forceinline__ float4 pack(const StageDesc &d, int l, const double x[6]) {
   const double s = d.rad[l];
   const double v = d.vol[l];
   const double rx = x[0] - d.ox, ry = x[1] - d.oy, rz = x[2] - d.oz;
   const float hx = (float)rx, hy = (float)ry, hz = (float)rz;
   const float ax = (float)x[3], ay = (float)x[4], az = (float)x[5];
-  d.pos32[l] = make_float4(hx, hy, hz, (float)(0.5 * s * s));
+  const float hw = (float)(0.5 * s * s);
+  d.pos32[l] = make_float4(hx, hy, hz, hw);
   d.poslo[l] = make_float4((float)(rx - (double)hx), (float)(ry - (double)hy),
                            (float)(rz - (double)hz), 0.f);
   d.vor32[l] = make_float4(ax, ay, az, (float)v);
@@ -35,26 +36,30 @@ __device__ __forceinline__ float3 pack(const StageDesc &d, int l, const double x
                            (float)(x[5] - (double)az), 0.f);
   d.pos64[l] = make_double4(x[0], x[1], x[2], s);
   d.vor64[l] = make_double4(x[3], x[4], x[5], v);
-  return make_float3(hx, hy, hz);
+  return make_float4(hx, hy, hz, hw);
 }
 
 // Bounding boxes of the block's tiles (box_tile particles each, aligned to
-// the segment); particles beyond n contribute nothing.
-__device__ __forceinline__ void tile_boxes(const StageDesc &d, int l0, float3 p, bool has) {
-  __shared__ float lo[3][kStageThreads];
-  __shared__ float hi[3][kStageThreads];
+// the segment); particles beyond n contribute nothing.  The box's w components
+// carry the tile's smallest (lo) and largest (hi) h = s^2/2, so the pair
+// kernel can tell tile pairs of one smoothing radius.
+__device__ __forceinline__ void tile_boxes(const StageDesc &d, int l0, float4 p, bool has) {
+  __shared__ float lo[4][kStageThreads];
+  __shared__ float hi[4][kStageThreads];
   const int t = threadIdx.x;
   lo[0][t] = has ? p.x : INFINITY;
   lo[1][t] = has ? p.y : INFINITY;
   lo[2][t] = has ? p.z : INFINITY;
+  lo[3][t] = has ? p.w : INFINITY;
   hi[0][t] = has ? p.x : -INFINITY;
   hi[1][t] = has ? p.y : -INFINITY;
   hi[2][t] = has ? p.z : -INFINITY;
+  hi[3][t] = has ? p.w : -INFINITY;
   __syncthreads();
   for (int s = d.box_tile / 2; s > 0; s >>= 1) {
     if ((t % d.box_tile) < s) {
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
+      for (int k = 0; k < 4; ++k) {
         lo[k][t] = fminf(lo[k][t], lo[k][t + s]);
         hi[k][t] = fmaxf(hi[k][t], hi[k][t + s]);
       }
@@ -63,8 +68,8 @@ __device__ __forceinline__ void tile_boxes(const StageDesc &d, int l0, float3 p,
   }
   if ((t % d.box_tile) == 0 && l0 + t < d.n) {
     const int b = (l0 + t) / d.box_tile;
-    d.boxes[2 * b] = make_float4(lo[0][t], lo[1][t], lo[2][t], 0.f);
-    d.boxes[2 * b + 1] = make_float4(hi[0][t], hi[1][t], hi[2][t], 0.f);
+    d.boxes[2 * b] = make_float4(lo[0][t], lo[1][t], lo[2][t], lo[3][t]);
+    d.boxes[2 * b + 1] = make_float4(hi[0][t], hi[1][t], hi[2][t], hi[3][t]);
   }
 }
 
@@ -145,7 +150,7 @@ __global__ void __launch_bounds__(kStageThreads)
       for (int k = 0; k < 6; ++k) x[k] = d.X[idx[k]];
     }
   }
-  float3 p = make_float3(0.f, 0.f, 0.f);
+  float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
   if (has) p = pack(d, l, x);
   tile_boxes(d, it.l0, p, has);
 }
