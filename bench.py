@@ -55,7 +55,18 @@ def parse():
     ap.add_argument("--no-suite", action="store_true", help="skip the batch and serving legs")
     ap.add_argument("--configs", action="store_true",
                     help="run every workload at its full length instead (minutes; one JSON line each)")
+    ap.add_argument("--tile", default=None,
+                    help="fixed FP32 tiling instead of the autotuned one: threads,threads_per_target,"
+                         "targets_per_thread,unroll,blocks_per_sm,packed[,items_per_slot]")
     return ap.parse_args()
+
+
+def apply_tile(s, spec: str):
+    v = [int(x) for x in spec.split(",")]
+    tb, p, r, unroll, minb, packed = v[:6]
+    ips = v[6] if len(v) > 6 else 32
+    s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=bool(packed))
+    return s.get_config()
 
 
 # ------------------------------------------------------------------ ranks
@@ -367,7 +378,10 @@ def run_pawan(args, rk: Ranks):
     ctx = Context(rk.local)
     info = ctx.info()
     s = System.from_scenario(ctx, sc, "f32")
-    tuned = s.get_config() if args.quick else s.autotune()
+    if args.tile:
+        tuned = apply_tile(s, args.tile)
+    else:
+        tuned = s.get_config() if args.quick else s.autotune()
     # Every step starts from the specified geometry: under the reference's
     # kernel this configuration scrambles within a few steps (the jittered near
     # field moves particles many station spacings per step), which would

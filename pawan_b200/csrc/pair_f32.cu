@@ -218,76 +218,103 @@ __device__ __forceinline__ void tile_far(const float4 *__restrict__ sa,
 }
 
 // ---- packed far path: two sources per FP32x2 instruction -----------------
-// Shared-memory layout of a source tile for it, per source pair k = (2k, 2k+1):
-//   f0[k] = (-x_2k, -x_2k+1, -y_2k, -y_2k+1)   f1[k] = (-z_2k, -z_2k+1, h_2k, h_2k+1)
-//   f2[k] = (ax_2k, ax_2k+1, ay_2k, ay_2k+1)   f3[k] = (az_2k, az_2k+1, v_2k, v_2k+1)
-// so a float4 load yields two operand pairs and the target enters every
-// instruction as a broadcast pair held in registers.
+// The far formulation above with every FP32 operation on a pair of sources
+// (FFMA2/FMUL2/FADD2 issue once for two lanes' worth of work, halving the
+// issue slots the FMA pipe needs).  Shared-memory layout of a far tile, per
+// source pair k = (a, b) = (2k, 2k+1):
+//   f0[k] = (-x'_a, -x'_b, -y'_a, -y'_b)   f1[k] = (-z'_a, -z'_b, h_a, h_b)
+//   f2[k] = (ax_a, ax_b, ay_a, ay_b)       f3[k] = (az_a, az_b, v_a, v_b)
+//   f4[k] = (bx_a, bx_b, by_a, by_b)       f5[k] = (bz_a, bz_b)   (beta = alpha x x')
+// so every load yields operand pairs and the target enters each instruction
+// as a broadcast pair held in registers.  Signs are arranged so that no
+// operand needs negating in the loop (a negated pair costs two scalar
+// instructions): positions are stored negated, the target's strength is held
+// negated, and the loop accumulates -fh.
 
 struct Acc2 {
-  float2 ux, uy, uz;
-  float2 qx, qy, qz;  // sum -qh alpha_j   (signs folded into the per-tile fold)
-  float2 gx, gy, gz;
-  float2 ex, ey, ez;
-  float2 ev;
+  float2 wx, wy, wz;  // sum qh beta_j
+  float2 qx, qy, qz;  // sum qh alpha_j
+  float2 gx, gy, gz;  // sum -fh t d
+  float2 ex, ey, ez;  // sum Dp alpha_j
+  float2 ev;          // sum Dp v_j
 };
 
 struct Target2 {
-  float2 x, y, z, h;  // broadcast (value, value)
-  float2 a, b, c;     // strength hi, broadcast
+  float2 x, y, z;     // x'_i, broadcast
+  float2 h;           // h_i, broadcast
+  float2 na, nb, nc;  // -alpha_i (hi), broadcast
+  float2 gx, gy, gz;  // gamma_i = x'_i x alpha_i, broadcast
 };
 
 __device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
-__device__ __forceinline__ float2 neg2(float2 v) { return make_float2(-v.x, -v.y); }
 
-template <bool DIFF, int NSRC, int U>
+template <bool DIFF, bool UNI, int NSRC, int U>
 __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
                                                 const float4 *__restrict__ f1,
                                                 const float4 *__restrict__ f2,
-                                                const float4 *__restrict__ f3, const Target2 &T,
-                                                Acc2 &a) {
+                                                const float4 *__restrict__ f3,
+                                                const float4 *__restrict__ f4,
+                                                const float2 *__restrict__ f5, const Target2 &T,
+                                                float hu, Acc2 &a) {
+  const float2 s2u = bc2(2.f * hu), h2 = bc2(hu), c240 = bc2(-480.f * hu);
 #pragma unroll U
   for (int k = 0; k < NSRC / 2; ++k) {
-    const float4 A0 = f0[k], A1 = f1[k], A2 = f2[k], A3 = f3[k];
+    const float4 A0 = f0[k], A1 = f1[k], A2 = f2[k], A3 = f3[k], A4 = f4[k];
+    const float2 bz = f5[k];
     const float2 npx = make_float2(A0.x, A0.y), npy = make_float2(A0.z, A0.w);
     const float2 npz = make_float2(A1.x, A1.y), hj = make_float2(A1.z, A1.w);
     const float2 sx = make_float2(A2.x, A2.y), sy = make_float2(A2.z, A2.w);
     const float2 sz = make_float2(A3.x, A3.y), sv = make_float2(A3.z, A3.w);
+    const float2 bx = make_float2(A4.x, A4.y), by = make_float2(A4.z, A4.w);
     const float2 dx = __fadd2_rn(T.x, npx);
     const float2 dy = __fadd2_rn(T.y, npy);
     const float2 dz = __fadd2_rn(T.z, npz);
     const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-    const float2 sig2 = __fadd2_rn(T.h, hj);
-    const float2 sr = __fadd2_rn(r2, sig2);
-    const float2 w = make_float2(rsqrtf(sr.x), rsqrtf(sr.y));
-    const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-    // kernel_scalars() in pairs, with qn = -qh
-    const float2 w2 = __fmul2_rn(w, w);
-    const float2 uu = __fmul2_rn(sig2, w2);
-    const float2 vv = __fmul2_rn(uu, w);
-    const float2 v2 = __fmul2_rn(vv, vv);
-    const float2 v4 = __fmul2_rn(v2, v2);
-    const float2 dp = __fmul2_rn(v4, vv);
-    const float2 zc = __fmul2_rn(dp, sig2);
-    const float2 nph = __fmul2_rn(__fmul2_rn(__ffma2_rn(bc2(-0.5f), uu, bc2(-1.0f)), w2), ri);
-    const float2 ri2 = __fmul2_rn(ri, ri);
-    const float2 qn = __fmul2_rn(__fmul2_rn(__ffma2_rn(bc2(7.5f), zc, nph), sig2), ri2);
-    const float2 fh = __fmul2_rn(__ffma2_rn(bc2(2.5f), zc, qn), ri2);
-    // c = alpha_j x d
-    const float2 cx = __ffma2_rn(sy, dz, neg2(__fmul2_rn(sz, dy)));
-    const float2 cy = __ffma2_rn(sz, dx, neg2(__fmul2_rn(sx, dz)));
-    const float2 cz = __ffma2_rn(sx, dy, neg2(__fmul2_rn(sy, dx)));
-    const float2 t = __ffma2_rn(T.c, cz, __ffma2_rn(T.b, cy, __fmul2_rn(T.a, cx)));
-    const float2 ft = __fmul2_rn(fh, t);
-    a.ux = __ffma2_rn(qn, cx, a.ux);
-    a.uy = __ffma2_rn(qn, cy, a.uy);
-    a.uz = __ffma2_rn(qn, cz, a.uz);
-    a.qx = __ffma2_rn(qn, sx, a.qx);
-    a.qy = __ffma2_rn(qn, sy, a.qy);
-    a.qz = __ffma2_rn(qn, sz, a.qz);
-    a.gx = __ffma2_rn(ft, dx, a.gx);
-    a.gy = __ffma2_rn(ft, dy, a.gy);
-    a.gz = __ffma2_rn(ft, dz, a.gz);
+    float2 qh, nfh, dp;
+    if (UNI) {
+      // kernel_scalars_uniform in pairs, returning -fs
+      const float2 sr = __fadd2_rn(r2, s2u);
+      const float2 w = make_float2(rsqrtf(sr.x), rsqrtf(sr.y));
+      const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+      const float2 ri2 = make_float2(rcp_approx(r2.x), rcp_approx(r2.y));
+      const float2 y = __fmul2_rn(w, w);
+      const float2 u = __fmul2_rn(h2, y);
+      const float2 v = __fmul2_rn(u, w);
+      const float2 v2 = __fmul2_rn(v, v);
+      dp = __fmul2_rn(__fmul2_rn(v2, v2), v);
+      const float2 ph = __fmul2_rn(__ffma2_rn(u, y, y), ri);
+      qh = __fmul2_rn(__ffma2_rn(c240, dp, ph), ri2);
+      nfh = __fmul2_rn(__ffma2_rn(bc2(-80.f), dp, qh), ri2);
+    } else {
+      // kernel_scalars in pairs, returning -fh
+      const float2 sig2 = __fadd2_rn(T.h, hj);
+      const float2 sr = __fadd2_rn(r2, sig2);
+      const float2 w = make_float2(rsqrtf(sr.x), rsqrtf(sr.y));
+      const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+      const float2 w2 = __fmul2_rn(w, w);
+      const float2 uu = __fmul2_rn(sig2, w2);
+      const float2 v = __fmul2_rn(uu, w);
+      const float2 v2 = __fmul2_rn(v, v);
+      dp = __fmul2_rn(__fmul2_rn(v2, v2), v);
+      const float2 zc = __fmul2_rn(dp, sig2);
+      const float2 ph = __fmul2_rn(__fmul2_rn(__ffma2_rn(bc2(0.5f), uu, bc2(1.0f)), w2), ri);
+      const float2 ri2 = __fmul2_rn(ri, ri);
+      qh = __fmul2_rn(__fmul2_rn(__ffma2_rn(bc2(-7.5f), zc, ph), sig2), ri2);
+      nfh = __fmul2_rn(__ffma2_rn(bc2(-2.5f), zc, qh), ri2);
+    }
+    // alpha_i.(alpha_j x d) = alpha_j.gamma_i - alpha_i.beta_j
+    const float2 t = __ffma2_rn(T.nc, bz, __ffma2_rn(T.nb, by, __ffma2_rn(T.na, bx,
+                     __ffma2_rn(sz, T.gz, __ffma2_rn(sy, T.gy, __fmul2_rn(sx, T.gx))))));
+    const float2 nft = __fmul2_rn(nfh, t);
+    a.wx = __ffma2_rn(qh, bx, a.wx);
+    a.wy = __ffma2_rn(qh, by, a.wy);
+    a.wz = __ffma2_rn(qh, bz, a.wz);
+    a.qx = __ffma2_rn(qh, sx, a.qx);
+    a.qy = __ffma2_rn(qh, sy, a.qy);
+    a.qz = __ffma2_rn(qh, sz, a.qz);
+    a.gx = __ffma2_rn(nft, dx, a.gx);
+    a.gy = __ffma2_rn(nft, dy, a.gy);
+    a.gz = __ffma2_rn(nft, dz, a.gz);
     if (DIFF) {
       a.ex = __ffma2_rn(dp, sx, a.ex);
       a.ey = __ffma2_rn(dp, sy, a.ey);
@@ -419,7 +446,8 @@ __global__ void __launch_bounds__(TB, MINB)
   __shared__ float4 sv[2][TB];
   __shared__ float4 spl[2][TB];
   __shared__ float4 svl[2][TB];
-  __shared__ float4 fq[4][2][FQ];
+  __shared__ float4 fq[5][2][FQ];
+  __shared__ float2 fz[2][FQ];
   __shared__ int s_item;
   const int tid = threadIdx.x;
   const int g = tid % P;
@@ -458,17 +486,6 @@ __global__ void __launch_bounds__(TB, MINB)
       for (int k = 0; k < 3; ++k) ou[r][k] = oa[r][k] = 0.0;
     }
 
-    Target2 T2;
-    if (PK) {
-      T2.x = bc2(T[0].xh);
-      T2.y = bc2(T[0].yh);
-      T2.z = bc2(T[0].zh);
-      T2.h = bc2(T[0].h);
-      T2.a = bc2(T[0].ah);
-      T2.b = bc2(T[0].bh);
-      T2.c = bc2(T[0].ch);
-    }
-
     // box of the target tile: union of the source-tile boxes it covers (w:
     // range of h)
     float4 tlo = __ldg(sg.boxes + 2 * (w.t0 / TB));
@@ -502,27 +519,34 @@ __global__ void __launch_bounds__(TB, MINB)
       // it in the far format (or the packed one); the barrier publishes the
       // tile and retires the previous one, whose buffer the next copies reuse
       wait_staged();
-      if (PK) {
-        const float4 p0 = sp[buf][tid], p1 = sv[buf][tid];
-        const int k = tid >> 1, hf = tid & 1;
-        float *q0 = reinterpret_cast<float *>(&fq[0][buf][k]);
-        float *q1 = reinterpret_cast<float *>(&fq[1][buf][k]);
-        float *q2 = reinterpret_cast<float *>(&fq[2][buf][k]);
-        float *q3 = reinterpret_cast<float *>(&fq[3][buf][k]);
-        q0[hf] = -p0.x;
-        q0[2 + hf] = -p0.y;
-        q1[hf] = -p0.z;
-        q1[2 + hf] = p0.w;
-        q2[hf] = p1.x;
-        q2[2 + hf] = p1.y;
-        q3[hf] = p1.z;
-        q3[2 + hf] = p1.w;
-      } else if (!near) {
+      if (!near) {
         const float4 p0 = sp[buf][tid], p1 = sv[buf][tid];
         const float px = p0.x - cx, py = p0.y - cy, pz = p0.z - cz;
-        sp[buf][tid] = make_float4(px, py, pz, p0.w);
-        spl[buf][tid] = make_float4(fmaf(p1.y, pz, -p1.z * py), fmaf(p1.z, px, -p1.x * pz),
-                                    fmaf(p1.x, py, -p1.y * px), 0.f);
+        const float bx = fmaf(p1.y, pz, -p1.z * py), by = fmaf(p1.z, px, -p1.x * pz),
+                    bz = fmaf(p1.x, py, -p1.y * px);
+        if (PK) {
+          const int k = tid >> 1, hf = tid & 1;
+          float *q0 = reinterpret_cast<float *>(&fq[0][buf][k]);
+          float *q1 = reinterpret_cast<float *>(&fq[1][buf][k]);
+          float *q2 = reinterpret_cast<float *>(&fq[2][buf][k]);
+          float *q3 = reinterpret_cast<float *>(&fq[3][buf][k]);
+          float *q4 = reinterpret_cast<float *>(&fq[4][buf][k]);
+          float *q5 = reinterpret_cast<float *>(&fz[buf][k]);
+          q0[hf] = -px;
+          q0[2 + hf] = -py;
+          q1[hf] = -pz;
+          q1[2 + hf] = p0.w;
+          q2[hf] = p1.x;
+          q2[2 + hf] = p1.y;
+          q3[hf] = p1.z;
+          q3[2 + hf] = p1.w;
+          q4[hf] = bx;
+          q4[2 + hf] = by;
+          q5[hf] = bz;
+        } else {
+          sp[buf][tid] = make_float4(px, py, pz, p0.w);
+          spl[buf][tid] = make_float4(bx, by, bz, 0.f);
+        }
       }
       __syncthreads();
       if (t + 1 < ntiles)
@@ -539,23 +563,44 @@ __global__ void __launch_bounds__(TB, MINB)
         az[r] = (double)T[r].ch + (double)cl[r];
       }
       if (!near && PK) {
+        Target2 T2;
+        const float fx = T[0].xh - cx, fy = T[0].yh - cy, fzz = T[0].zh - cz;
+        T2.x = bc2(fx);
+        T2.y = bc2(fy);
+        T2.z = bc2(fzz);
+        T2.h = bc2(T[0].h);
+        T2.na = bc2(-T[0].ah);
+        T2.nb = bc2(-T[0].bh);
+        T2.nc = bc2(-T[0].ch);
+        T2.gx = bc2(fmaf(fy, T[0].ch, -fzz * T[0].bh));
+        T2.gy = bc2(fmaf(fzz, T[0].ah, -fx * T[0].ch));
+        T2.gz = bc2(fmaf(fx, T[0].bh, -fy * T[0].ah));
         Acc2 b;
-        b.ux = b.uy = b.uz = b.qx = b.qy = b.qz = b.gx = b.gy = b.gz = make_float2(0.f, 0.f);
+        b.wx = b.wy = b.wz = b.qx = b.qy = b.qz = b.gx = b.gy = b.gz = make_float2(0.f, 0.f);
         b.ex = b.ey = b.ez = b.ev = make_float2(0.f, 0.f);
-        tile_far_packed<DIFF, TB, U>(fq[0][buf], fq[1][buf], fq[2][buf], fq[3][buf], T2, b);
-        const double Qx = -A * (b.qx.x + b.qx.y), Qy = -A * (b.qy.x + b.qy.y),
-                     Qz = -A * (b.qz.x + b.qz.y);
-        ou[0][0] -= A * (b.ux.x + b.ux.y);
-        ou[0][1] -= A * (b.uy.x + b.uy.y);
-        ou[0][2] -= A * (b.uz.x + b.uz.y);
-        oa[0][0] += (ay[0] * Qz - az[0] * Qy) + 3.0 * A * (b.gx.x + b.gx.y);
-        oa[0][1] += (az[0] * Qx - ax[0] * Qz) + 3.0 * A * (b.gy.x + b.gy.y);
-        oa[0][2] += (ax[0] * Qy - ay[0] * Qx) + 3.0 * A * (b.gz.x + b.gz.y);
+        if (uni)
+          tile_far_packed<DIFF, true, TB, U>(fq[0][buf], fq[1][buf], fq[2][buf], fq[3][buf],
+                                             fq[4][buf], fz[buf], T2, slo.w, b);
+        else
+          tile_far_packed<DIFF, false, TB, U>(fq[0][buf], fq[1][buf], fq[2][buf], fq[3][buf],
+                                              fq[4][buf], fz[buf], T2, 0.f, b);
+        const double s2 = uni ? 2.0 * (double)slo.w : 1.0;
+        const double As2 = A * s2;
+        const double cd = uni ? 32.0 * cnu : cnu;
+        const double Qx = As2 * (b.qx.x + b.qx.y), Qy = As2 * (b.qy.x + b.qy.y),
+                     Qz = As2 * (b.qz.x + b.qz.y);
+        const double xp = fx, yp = fy, zp = fzz;
+        ou[0][0] += (Qy * zp - Qz * yp) - As2 * (b.wx.x + b.wx.y);
+        ou[0][1] += (Qz * xp - Qx * zp) - As2 * (b.wy.x + b.wy.y);
+        ou[0][2] += (Qx * yp - Qy * xp) - As2 * (b.wz.x + b.wz.y);
+        oa[0][0] += (ay[0] * Qz - az[0] * Qy) - 3.0 * As2 * (b.gx.x + b.gx.y);
+        oa[0][1] += (az[0] * Qx - ax[0] * Qz) - 3.0 * As2 * (b.gy.x + b.gy.y);
+        oa[0][2] += (ax[0] * Qy - ay[0] * Qx) - 3.0 * As2 * (b.gz.x + b.gz.y);
         if (DIFF) {
           const double v = T[0].v, ev = b.ev.x + b.ev.y;
-          oa[0][0] += cnu * (v * (b.ex.x + b.ex.y) - ev * ax[0]);
-          oa[0][1] += cnu * (v * (b.ey.x + b.ey.y) - ev * ay[0]);
-          oa[0][2] += cnu * (v * (b.ez.x + b.ez.y) - ev * az[0]);
+          oa[0][0] += cd * (v * (b.ex.x + b.ex.y) - ev * ax[0]);
+          oa[0][1] += cd * (v * (b.ey.x + b.ey.y) - ev * ay[0]);
+          oa[0][2] += cd * (v * (b.ez.x + b.ez.y) - ev * az[0]);
         }
       } else if (!near) {
         FarTarget F[R];
@@ -666,6 +711,7 @@ KernelFn select(const PairConfig &c) {
 #define PAWAN_F32_CASE(TB_, P_, R_, U_, MINB_) PAWAN_F32_CASE_PK(TB_, P_, R_, U_, MINB_, false)
   PAWAN_F32_CASE_PK(128, 1, 1, 1, 4, true)
   PAWAN_F32_CASE_PK(128, 1, 1, 2, 4, true)
+  PAWAN_F32_CASE_PK(128, 1, 1, 4, 4, true)
   PAWAN_F32_CASE_PK(128, 1, 1, 1, 5, true)
   PAWAN_F32_CASE_PK(128, 1, 1, 2, 5, true)
   PAWAN_F32_CASE(128, 1, 1, 2, 4)

@@ -42,7 +42,7 @@ int cuda_fail(pawan_ctx *ctx, cudaError_t e, const char *where) {
 TileChoice default_tile(int precision) {
   TileChoice t;
   if (precision == PAWAN_PREC_F32) {
-    t.pc = PairConfig{256, 1, 1, 2};
+    t.pc = PairConfig{128, 1, 4, 1, 0, true};  // packed far path, unroll 4
   } else {
     t.pc = PairConfig{128, 1, 1};
   }
@@ -59,7 +59,8 @@ std::vector<TileChoice> tile_candidates(int precision) {
     // some workload (threads per target > 1 for small systems, two targets
     // per thread or packed pairs for large ones)
     const int shapes[][5] = {{1, 1, 4, 0, 0}, {2, 1, 4, 0, 0}, {4, 1, 4, 0, 0}, {1, 2, 1, 0, 0},
-                             {1, 2, 2, 0, 0}, {1, 1, 4, 5, 0}, {1, 1, 2, 0, 1}, {1, 1, 2, 5, 1}};
+                             {1, 2, 2, 0, 0}, {1, 1, 4, 5, 0}, {1, 1, 1, 0, 1}, {1, 1, 2, 0, 1},
+                             {1, 1, 4, 0, 1}, {1, 1, 2, 5, 1}};
     for (int tb : {128, 256})
       for (const auto &sh : shapes) {
         TileChoice t;

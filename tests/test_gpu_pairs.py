@@ -95,7 +95,7 @@ F32_TILINGS = [(128, 1, 1, 2, 0), (128, 1, 1, 4, 0), (128, 2, 1, 2, 0), (128, 2,
                (256, 1, 1, 4, 0), (256, 2, 1, 4, 0), (256, 4, 1, 4, 0), (256, 1, 2, 1, 0),
                (256, 1, 2, 2, 0), (256, 1, 1, 4, 3)]
 # packed far path (two sources per FP32x2 instruction): (threads, unroll, blocks per SM)
-F32_PACKED = [(128, 1, 0), (128, 2, 0), (128, 1, 5), (128, 2, 5)]
+F32_PACKED = [(128, 1, 0), (128, 2, 0), (128, 4, 0), (128, 1, 5), (128, 2, 5)]
 
 
 @pytest.mark.parametrize("tb,unroll,minb", F32_PACKED)
@@ -125,6 +125,43 @@ def test_every_f32_tiling(ctx, tb, p, r, unroll, minb):
     s.set_nu(0.0)
     s.solve()
     check("f32", *s.union_rates(), *oracle.pairs(pos, vor, rad, vol, 0.0))
+
+
+def _separated_rings(alternate: bool):
+    """Three rings far apart (most tile pairs take the far formulation), the
+    second with a larger smoothing radius; with `alternate` the third ring's
+    particles alternate between two radii (no uniform-radius tile pairs)."""
+    rng = np.random.default_rng(77)
+    wakes = [g.ring(1.0, 0.1, 1.0, 48, 0.0, rng), g.ring(0.8, 0.1, -0.7, 40, 3.0, rng),
+             g.ring(1.2, 0.08, 1.3, 56, -2.5, rng)]
+    wakes[1].rad *= 1.3
+    if alternate:
+        wakes[2].rad[1::2] *= 0.7
+    counts = [w.n for w in wakes]
+    pos = np.concatenate([w.pos for w in wakes])
+    vor = np.concatenate([w.vor for w in wakes])
+    rad = np.concatenate([w.rad for w in wakes])
+    vol = np.concatenate([w.vol for w in wakes])
+    return counts, pos, vor, rad, vol
+
+
+@pytest.mark.parametrize("alternate", [False, True])
+def test_far_formulations_every_tiling(ctx, alternate):
+    """Uniform-radius and mixed-radius far tiles, scalar and packed paths."""
+    counts, pos, vor, rad, vol = _separated_rings(alternate)
+    s = System(ctx, counts, 1e-3, "f32")
+    s.set_particles(pos, vor, rad, vol)
+    for nu in (1e-3, 0.0):
+        s.set_nu(nu)
+        u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, nu)
+        for tb, p, r, unroll, minb in F32_TILINGS:
+            s.set_config(tb, p, unroll, 16, targets_per_thread=r, blocks_per_sm=minb)
+            s.solve()
+            check("f32", *s.union_rates(), u_ref, da_ref)
+        for tb, unroll, minb in F32_PACKED:
+            s.set_config(tb, 1, unroll, 16, blocks_per_sm=minb, packed=True)
+            s.solve()
+            check("f32", *s.union_rates(), u_ref, da_ref)
 
 
 def test_nu_zero_matches_and_set_nu(ctx):
