@@ -65,7 +65,7 @@ def apply_tile(s, spec: str):
     v = [int(x) for x in spec.split(",")]
     tb, p, r, unroll, minb, packed = v[:6]
     ips = v[6] if len(v) > 6 else 32
-    s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=bool(packed))
+    s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=packed)
     return s.get_config()
 
 

@@ -52,7 +52,9 @@ typedef struct {
   int unroll;             /* unroll depth of the source loop */
   int blocks_per_sm;      /* blocks per SM the registers are bounded for, 0 = default */
   int items_per_slot;     /* work items per resident block (source chunking) */
-  int packed;             /* 1: far tiles two sources per FP32x2 instruction */
+  int packed;             /* far tiles two sources per FP32x2 instruction: 1 with
+                             1/rho^2 from the MUFU reciprocal, 2 from rsqrt
+                             squared; 0: one source per instruction */
 } pawan_tiling;
 
 typedef struct pawan_ctx pawan_ctx;

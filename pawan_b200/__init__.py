@@ -60,9 +60,12 @@ class Tiling(ctypes.Structure):
 
 
 def _tiling(threads, threads_per_target=1, unroll=4, items_per_slot=16, targets_per_thread=1,
-            blocks_per_sm=0, packed=False) -> Tiling:
+            blocks_per_sm=0, packed=0) -> Tiling:
+    """packed: 0 one source per instruction on far tiles; 1 two sources per FP32x2
+    instruction with 1/rho^2 from the MUFU reciprocal; 2 the same with 1/rho^2
+    from rsqrt squared (True means 1)."""
     return Tiling(threads, threads_per_target, targets_per_thread, unroll, blocks_per_sm, items_per_slot,
-                  1 if packed else 0)
+                  int(packed))
 
 
 class ServeStats(ctypes.Structure):
@@ -372,7 +375,7 @@ class System:
 
     def set_config(self, threads: int, threads_per_target: int = 1, unroll: int = 4,
                    items_per_slot: int = 16, targets_per_thread: int = 1, blocks_per_sm: int = 0,
-                   packed: bool = False):
+                   packed: int = 0):
         t = _tiling(threads, threads_per_target, unroll, items_per_slot, targets_per_thread, blocks_per_sm,
                     packed)
         self.ctx.check(self._lib.pawan_system_set_tiling(self._h, ctypes.byref(t)))
@@ -431,7 +434,7 @@ class Batch:
 
     def set_config(self, threads: int, threads_per_target: int = 1, unroll: int = 4,
                    items_per_slot: int = 16, targets_per_thread: int = 1, blocks_per_sm: int = 0,
-                   packed: bool = False):
+                   packed: int = 0):
         t = _tiling(threads, threads_per_target, unroll, items_per_slot, targets_per_thread, blocks_per_sm,
                     packed)
         self.ctx.check(self._lib.pawan_batch_set_tiling(self._h, ctypes.byref(t)))

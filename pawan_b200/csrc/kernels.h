@@ -11,14 +11,16 @@ namespace pawan {
 // shared-memory tile), `p` threads per target, `r` targets per thread
 // (targets per block = tb / p * r), `unroll` = unroll depth of the source loop,
 // `minb` = blocks per SM the registers are bounded for (0: the default),
-// `packed` = far tiles computed two sources per FP32x2 instruction.
+// `packed` = far tiles computed two sources per FP32x2 instruction (1: 1/rho^2
+// from the MUFU reciprocal on uniform-radius tiles, 2: from rsqrt squared;
+// 0: one source per instruction).
 struct PairConfig {
   int tb;
   int p;
   int unroll;
   int r = 1;
   int minb = 0;
-  bool packed = false;
+  int packed = 0;
 };
 
 inline int targets_per_block(const PairConfig &c) { return c.tb / c.p * c.r; }

@@ -60,6 +60,10 @@
 // current one.  The result of an item (u, dalpha in
 // FP64) goes to its chunk of the partial buffer, which the stage kernel
 // reduces in chunk order.
+#include <mutex>
+#include <set>
+#include <utility>
+
 #include "device.cuh"
 #include "kernels.h"
 
@@ -248,7 +252,7 @@ struct Target2 {
 
 __device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
 
-template <bool DIFF, bool UNI, int NSRC, int U>
+template <bool DIFF, bool UNI, bool RCP, int NSRC, int U>
 __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
                                                 const float4 *__restrict__ f1,
                                                 const float4 *__restrict__ f2,
@@ -276,7 +280,9 @@ __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
       const float2 sr = __fadd2_rn(r2, s2u);
       const float2 w = make_float2(rsqrtf(sr.x), rsqrtf(sr.y));
       const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-      const float2 ri2 = make_float2(rcp_approx(r2.x), rcp_approx(r2.y));
+      // 1/rho^2 from the MUFU reciprocal (RCP) or from one FMA-pipe multiply:
+      // which pipe has room depends on the instruction mix around the loop
+      const float2 ri2 = RCP ? make_float2(rcp_approx(r2.x), rcp_approx(r2.y)) : __fmul2_rn(ri, ri);
       const float2 y = __fmul2_rn(w, w);
       const float2 u = __fmul2_rn(h2, y);
       const float2 v = __fmul2_rn(u, w);
@@ -432,22 +438,28 @@ __device__ __forceinline__ bool far_tiles(float4 tlo, float4 thi, float4 slo, fl
 
 // Threads per target P > 1 split a tile's sources (R = 1); targets per thread
 // R > 1 reuse each source loaded from shared memory for R targets (P = 1);
-// PK: the far path processes two sources per FP32x2 instruction (P = R = 1).
+// PK > 0: the far path processes two sources per FP32x2 instruction (P = R =
+// 1), taking 1/rho^2 on uniform-radius tiles from the MUFU reciprocal (PK = 1)
+// or from rsqrt squared (PK = 2).
 // MINB: blocks per SM the register allocation is bounded for (occupancy).
-template <int TB, int P, int R, int U, bool DIFF, int MINB, bool PK>
+template <int TB, int P, int R, int U, bool DIFF, int MINB, int PK>
 __global__ void __launch_bounds__(TB, MINB)
     pairs_f32_kernel(const WorkItem *__restrict__ items, int n_items,
                      const SegDesc *__restrict__ segs, int *__restrict__ next_item) {
-  static_assert(!PK || (P == 1 && R == 1), "the packed far path has one target per thread");
+  static_assert(PK == 0 || (P == 1 && R == 1), "the packed far path has one target per thread");
   constexpr int TG = TB / P;   // targets per block and per target row r
   constexpr int TPB = TG * R;  // targets per block
   constexpr int FQ = PK ? TB / 2 : 1;
-  __shared__ float4 sp[2][TB];
-  __shared__ float4 sv[2][TB];
-  __shared__ float4 spl[2][TB];
-  __shared__ float4 svl[2][TB];
-  __shared__ float4 fq[5][2][FQ];
-  __shared__ float2 fz[2][FQ];
+  // two-stage tile ring in dynamic shared memory (pair_f32_smem_bytes):
+  // sp, sv, spl, svl [2][TB] (pos32, vor32, poslo, vorlo as staged), then
+  // the packed far format fq [5][2][FQ] float4 and fz [2][FQ] float2
+  extern __shared__ float4 smem_f32[];
+  float4 *const sp = smem_f32;
+  float4 *const sv = sp + 2 * TB;
+  float4 *const spl = sv + 2 * TB;
+  float4 *const svl = spl + 2 * TB;
+  float4 *const fq = svl + 2 * TB;
+  float2 *const fz = reinterpret_cast<float2 *>(fq + 10 * FQ);
   __shared__ int s_item;
   const int tid = threadIdx.x;
   const int g = tid % P;
@@ -503,7 +515,7 @@ __global__ void __launch_bounds__(TB, MINB)
     }
 
     const int ntiles = (w.s1 - w.s0 + TB - 1) / TB;
-    stage_source(sg, w.s0 + tid, w.s1, &sp[0][tid], &sv[0][tid], &spl[0][tid], &svl[0][tid]);
+    stage_source(sg, w.s0 + tid, w.s1, sp + tid, sv + tid, spl + tid, svl + tid);
     for (int t = 0; t < ntiles; ++t) {
       const int buf = t & 1;
       const int ts = w.s0 + t * TB;
@@ -520,18 +532,18 @@ __global__ void __launch_bounds__(TB, MINB)
       // tile and retires the previous one, whose buffer the next copies reuse
       wait_staged();
       if (!near) {
-        const float4 p0 = sp[buf][tid], p1 = sv[buf][tid];
+        const float4 p0 = sp[buf * TB + tid], p1 = sv[buf * TB + tid];
         const float px = p0.x - cx, py = p0.y - cy, pz = p0.z - cz;
         const float bx = fmaf(p1.y, pz, -p1.z * py), by = fmaf(p1.z, px, -p1.x * pz),
                     bz = fmaf(p1.x, py, -p1.y * px);
         if (PK) {
           const int k = tid >> 1, hf = tid & 1;
-          float *q0 = reinterpret_cast<float *>(&fq[0][buf][k]);
-          float *q1 = reinterpret_cast<float *>(&fq[1][buf][k]);
-          float *q2 = reinterpret_cast<float *>(&fq[2][buf][k]);
-          float *q3 = reinterpret_cast<float *>(&fq[3][buf][k]);
-          float *q4 = reinterpret_cast<float *>(&fq[4][buf][k]);
-          float *q5 = reinterpret_cast<float *>(&fz[buf][k]);
+          float *q0 = reinterpret_cast<float *>(fq + (0 * 2 + buf) * FQ + k);
+          float *q1 = reinterpret_cast<float *>(fq + (1 * 2 + buf) * FQ + k);
+          float *q2 = reinterpret_cast<float *>(fq + (2 * 2 + buf) * FQ + k);
+          float *q3 = reinterpret_cast<float *>(fq + (3 * 2 + buf) * FQ + k);
+          float *q4 = reinterpret_cast<float *>(fq + (4 * 2 + buf) * FQ + k);
+          float *q5 = reinterpret_cast<float *>(fz + buf * FQ + k);
           q0[hf] = -px;
           q0[2 + hf] = -py;
           q1[hf] = -pz;
@@ -544,14 +556,14 @@ __global__ void __launch_bounds__(TB, MINB)
           q4[2 + hf] = by;
           q5[hf] = bz;
         } else {
-          sp[buf][tid] = make_float4(px, py, pz, p0.w);
-          spl[buf][tid] = make_float4(bx, by, bz, 0.f);
+          sp[buf * TB + tid] = make_float4(px, py, pz, p0.w);
+          spl[buf * TB + tid] = make_float4(bx, by, bz, 0.f);
         }
       }
       __syncthreads();
       if (t + 1 < ntiles)
-        stage_source(sg, ts + TB + tid, w.s1, &sp[buf ^ 1][tid], &sv[buf ^ 1][tid],
-                     &spl[buf ^ 1][tid], &svl[buf ^ 1][tid]);
+        stage_source(sg, ts + TB + tid, w.s1, sp + (buf ^ 1) * TB + tid, sv + (buf ^ 1) * TB + tid,
+                     spl + (buf ^ 1) * TB + tid, svl + (buf ^ 1) * TB + tid);
       Acc32 a[R];
 #pragma unroll
       for (int r = 0; r < R; ++r) a[r] = Acc32{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
@@ -579,11 +591,13 @@ __global__ void __launch_bounds__(TB, MINB)
         b.wx = b.wy = b.wz = b.qx = b.qy = b.qz = b.gx = b.gy = b.gz = make_float2(0.f, 0.f);
         b.ex = b.ey = b.ez = b.ev = make_float2(0.f, 0.f);
         if (uni)
-          tile_far_packed<DIFF, true, TB, U>(fq[0][buf], fq[1][buf], fq[2][buf], fq[3][buf],
-                                             fq[4][buf], fz[buf], T2, slo.w, b);
+          tile_far_packed<DIFF, true, PK == 1, TB, U>(fq + buf * FQ, fq + (2 + buf) * FQ,
+                                                      fq + (4 + buf) * FQ, fq + (6 + buf) * FQ,
+                                                      fq + (8 + buf) * FQ, fz + buf * FQ, T2, slo.w, b);
         else
-          tile_far_packed<DIFF, false, TB, U>(fq[0][buf], fq[1][buf], fq[2][buf], fq[3][buf],
-                                              fq[4][buf], fz[buf], T2, 0.f, b);
+          tile_far_packed<DIFF, false, PK == 1, TB, U>(fq + buf * FQ, fq + (2 + buf) * FQ,
+                                                       fq + (4 + buf) * FQ, fq + (6 + buf) * FQ,
+                                                       fq + (8 + buf) * FQ, fz + buf * FQ, T2, 0.f, b);
         const double s2 = uni ? 2.0 * (double)slo.w : 1.0;
         const double As2 = A * s2;
         const double cd = uni ? 32.0 * cnu : cnu;
@@ -614,9 +628,11 @@ __global__ void __launch_bounds__(TB, MINB)
           F[r].gz = fmaf(F[r].x, T[r].bh, -F[r].y * T[r].ah);
         }
         if (uni)
-          tile_far<DIFF, true, P, R, TB, U>(sp[buf], sv[buf], spl[buf], g, T, F, slo.w, a);
+          tile_far<DIFF, true, P, R, TB, U>(sp + buf * TB, sv + buf * TB, spl + buf * TB, g, T, F,
+                                            slo.w, a);
         else
-          tile_far<DIFF, false, P, R, TB, U>(sp[buf], sv[buf], spl[buf], g, T, F, 0.f, a);
+          tile_far<DIFF, false, P, R, TB, U>(sp + buf * TB, sv + buf * TB, spl + buf * TB, g, T, F,
+                                             0.f, a);
         // undo the uniform-radius scaling: qh = sigma^2 qs, fh = sigma^2 fs, Dp = 32 ds
         const double s2 = uni ? 2.0 * (double)slo.w : 1.0;
         const double As2 = A * s2;
@@ -649,11 +665,11 @@ __global__ void __launch_bounds__(TB, MINB)
           tvl[r] = valid[r] ? __ldg(sg.vorlo + ti[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         if (diag)
-          tile_near<DIFF, true, P, R, TB>(sp[buf], sv[buf], spl[buf], svl[buf], g, skip, T, tpl,
-                                          tvl, a);
+          tile_near<DIFF, true, P, R, TB>(sp + buf * TB, sv + buf * TB, spl + buf * TB,
+                                          svl + buf * TB, g, skip, T, tpl, tvl, a);
         else
-          tile_near<DIFF, false, P, R, TB>(sp[buf], sv[buf], spl[buf], svl[buf], g, skip, T, tpl,
-                                           tvl, a);
+          tile_near<DIFF, false, P, R, TB>(sp + buf * TB, sv + buf * TB, spl + buf * TB,
+                                           svl + buf * TB, g, skip, T, tpl, tvl, a);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
           ou[r][0] += A * a[r].ux;
@@ -708,12 +724,18 @@ KernelFn select(const PairConfig &c) {
   if (c.tb == TB_ && c.p == P_ && c.r == R_ && c.unroll == U_ && c.packed == PK_ &&      \
       (c.minb == MINB_ || (c.minb == 0 && MINB_ == (TB_ <= 128 ? 4 : 2))))              \
     return &pairs_f32_kernel<TB_, P_, R_, U_, DIFF, MINB_, PK_>;
-#define PAWAN_F32_CASE(TB_, P_, R_, U_, MINB_) PAWAN_F32_CASE_PK(TB_, P_, R_, U_, MINB_, false)
-  PAWAN_F32_CASE_PK(128, 1, 1, 1, 4, true)
-  PAWAN_F32_CASE_PK(128, 1, 1, 2, 4, true)
-  PAWAN_F32_CASE_PK(128, 1, 1, 4, 4, true)
-  PAWAN_F32_CASE_PK(128, 1, 1, 1, 5, true)
-  PAWAN_F32_CASE_PK(128, 1, 1, 2, 5, true)
+#define PAWAN_F32_CASE(TB_, P_, R_, U_, MINB_) PAWAN_F32_CASE_PK(TB_, P_, R_, U_, MINB_, 0)
+  PAWAN_F32_CASE_PK(128, 1, 1, 1, 4, 1)
+  PAWAN_F32_CASE_PK(128, 1, 1, 2, 4, 1)
+  PAWAN_F32_CASE_PK(128, 1, 1, 4, 4, 1)
+  PAWAN_F32_CASE_PK(128, 1, 1, 1, 5, 1)
+  PAWAN_F32_CASE_PK(128, 1, 1, 2, 5, 1)
+  PAWAN_F32_CASE_PK(128, 1, 1, 2, 4, 2)
+  PAWAN_F32_CASE_PK(128, 1, 1, 4, 4, 2)
+  PAWAN_F32_CASE_PK(256, 1, 1, 2, 2, 1)
+  PAWAN_F32_CASE_PK(256, 1, 1, 4, 2, 1)
+  PAWAN_F32_CASE_PK(256, 1, 1, 2, 2, 2)
+  PAWAN_F32_CASE_PK(256, 1, 1, 4, 2, 2)
   PAWAN_F32_CASE(128, 1, 1, 2, 4)
   PAWAN_F32_CASE(128, 1, 1, 4, 4)
   PAWAN_F32_CASE(128, 2, 1, 2, 4)
@@ -741,6 +763,27 @@ KernelFn select(const PairConfig &c, bool diffusion) {
   return diffusion ? select<true>(c) : select<false>(c);
 }
 
+// Dynamic shared memory of a tiling: the staged ring plus the packed far format.
+size_t smem_bytes(const PairConfig &c) {
+  const size_t fq = c.packed ? (size_t)c.tb / 2 : 1;
+  return 8 * (size_t)c.tb * sizeof(float4) + 10 * fq * sizeof(float4) + 2 * fq * sizeof(float2);
+}
+
+// Opts a kernel in to its dynamic shared memory beyond the default 48 KB (once
+// per kernel and device).
+cudaError_t prepare(KernelFn f, size_t bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<int, KernelFn>> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count({dev, f})) return cudaSuccess;
+  e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) done.insert({dev, f});
+  return e;
+}
+
 }  // namespace
 
 bool pairs_f32_supported(const PairConfig &c) { return select(c, true) != nullptr; }
@@ -748,14 +791,20 @@ bool pairs_f32_supported(const PairConfig &c) { return select(c, true) != nullpt
 cudaError_t pairs_f32_occupancy(const PairConfig &c, bool diffusion, int *blocks_per_sm) {
   KernelFn f = select(c, diffusion);
   if (!f) return cudaErrorInvalidValue;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, c.tb, 0);
+  const size_t bytes = smem_bytes(c);
+  cudaError_t e = prepare(f, bytes);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, c.tb, bytes);
 }
 
 cudaError_t launch_pairs_f32(const PairConfig &c, bool diffusion, int grid, const WorkItem *items,
                              int n_items, const SegDesc *segs, int *next_item, cudaStream_t s) {
   KernelFn f = select(c, diffusion);
   if (!f) return cudaErrorInvalidValue;
-  f<<<grid, c.tb, 0, s>>>(items, n_items, segs, next_item);
+  const size_t bytes = smem_bytes(c);
+  cudaError_t e = prepare(f, bytes);
+  if (e != cudaSuccess) return e;
+  f<<<grid, c.tb, bytes, s>>>(items, n_items, segs, next_item);
   return cudaGetLastError();
 }
 

@@ -42,7 +42,7 @@ int cuda_fail(pawan_ctx *ctx, cudaError_t e, const char *where) {
 TileChoice default_tile(int precision) {
   TileChoice t;
   if (precision == PAWAN_PREC_F32) {
-    t.pc = PairConfig{128, 1, 4, 1, 0, true};  // packed far path, unroll 4
+    t.pc = PairConfig{128, 1, 4, 1, 0, 1};  // packed far path, unroll 4
   } else {
     t.pc = PairConfig{128, 1, 1};
   }
@@ -60,11 +60,11 @@ std::vector<TileChoice> tile_candidates(int precision) {
     // per thread or packed pairs for large ones)
     const int shapes[][5] = {{1, 1, 4, 0, 0}, {2, 1, 4, 0, 0}, {4, 1, 4, 0, 0}, {1, 2, 1, 0, 0},
                              {1, 2, 2, 0, 0}, {1, 1, 4, 5, 0}, {1, 1, 1, 0, 1}, {1, 1, 2, 0, 1},
-                             {1, 1, 4, 0, 1}, {1, 1, 2, 5, 1}};
+                             {1, 1, 4, 0, 1}, {1, 1, 2, 5, 1}, {1, 1, 2, 0, 2}, {1, 1, 4, 0, 2}};
     for (int tb : {128, 256})
       for (const auto &sh : shapes) {
         TileChoice t;
-        t.pc = PairConfig{tb, sh[0], sh[2], sh[1], sh[3], sh[4] != 0};
+        t.pc = PairConfig{tb, sh[0], sh[2], sh[1], sh[3], sh[4]};
         if (pairs_f32_supported(t.pc)) v.push_back(t);
       }
   } else {
@@ -909,9 +909,9 @@ static int tile_from_abi(pawan_ctx *ctx, int precision, const pawan_tiling *t, T
   if (!t) return fail(ctx, PAWAN_ERR_INVALID, "null tiling");
   TileChoice c;
   c.pc = PairConfig{t->threads, t->threads_per_target, t->unroll, t->targets_per_thread,
-                    t->blocks_per_sm, t->packed != 0};
+                    t->blocks_per_sm, t->packed};
   c.items_per_slot = t->items_per_slot;
-  if (t->items_per_slot < 1 || t->targets_per_thread < 1 || t->blocks_per_sm < 0 ||
+  if (t->items_per_slot < 1 || t->targets_per_thread < 1 || t->blocks_per_sm < 0 || t->packed < 0 ||
       !tile_supported(precision, c.pc))
     return fail(ctx, PAWAN_ERR_INVALID, "tiling not compiled for this precision");
   *out = c;
@@ -935,7 +935,7 @@ int pawan_system_get_tiling(pawan_system *sys, pawan_tiling *tiling) {
   tiling->targets_per_thread = sys->tile.pc.r;
   tiling->unroll = sys->tile.pc.unroll;
   tiling->blocks_per_sm = sys->tile.pc.minb;
-  tiling->packed = sys->tile.pc.packed ? 1 : 0;
+  tiling->packed = sys->tile.pc.packed;
   tiling->items_per_slot = sys->tile.items_per_slot;
   return PAWAN_OK;
 }

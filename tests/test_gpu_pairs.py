@@ -94,12 +94,15 @@ F32_TILINGS = [(128, 1, 1, 2, 0), (128, 1, 1, 4, 0), (128, 2, 1, 2, 0), (128, 2,
                (128, 1, 1, 4, 5), (128, 1, 1, 2, 6), (128, 1, 1, 4, 6), (256, 1, 1, 2, 0),
                (256, 1, 1, 4, 0), (256, 2, 1, 4, 0), (256, 4, 1, 4, 0), (256, 1, 2, 1, 0),
                (256, 1, 2, 2, 0), (256, 1, 1, 4, 3)]
-# packed far path (two sources per FP32x2 instruction): (threads, unroll, blocks per SM)
-F32_PACKED = [(128, 1, 0), (128, 2, 0), (128, 4, 0), (128, 1, 5), (128, 2, 5)]
+# packed far path (two sources per FP32x2 instruction): (threads, unroll, blocks per SM,
+# mode: 1 = 1/rho^2 from the MUFU reciprocal, 2 = from rsqrt squared)
+F32_PACKED = [(128, 1, 0, 1), (128, 2, 0, 1), (128, 4, 0, 1), (128, 1, 5, 1), (128, 2, 5, 1),
+              (128, 2, 0, 2), (128, 4, 0, 2), (256, 2, 0, 1), (256, 4, 0, 1), (256, 2, 0, 2),
+              (256, 4, 0, 2)]
 
 
-@pytest.mark.parametrize("tb,unroll,minb", F32_PACKED)
-def test_every_packed_f32_tiling(ctx, tb, unroll, minb):
+@pytest.mark.parametrize("tb,unroll,minb,mode", F32_PACKED)
+def test_every_packed_f32_tiling(ctx, tb, unroll, minb, mode):
     sc = g.ring_pair(n_stations=70, seed=34, nu=1e-3)
     pos, vor, rad, vol = sc.union()
     s = System.from_scenario(ctx, sc, "f32")
@@ -107,7 +110,7 @@ def test_every_packed_f32_tiling(ctx, tb, unroll, minb):
         s.set_nu(nu)
         u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, nu)
         for ips in (1, 16, 64):
-            s.set_config(tb, 1, unroll, ips, blocks_per_sm=minb, packed=True)
+            s.set_config(tb, 1, unroll, ips, blocks_per_sm=minb, packed=mode)
             s.solve()
             check("f32", *s.union_rates(), u_ref, da_ref)
 
@@ -158,8 +161,8 @@ def test_far_formulations_every_tiling(ctx, alternate):
             s.set_config(tb, p, unroll, 16, targets_per_thread=r, blocks_per_sm=minb)
             s.solve()
             check("f32", *s.union_rates(), u_ref, da_ref)
-        for tb, unroll, minb in F32_PACKED:
-            s.set_config(tb, 1, unroll, 16, blocks_per_sm=minb, packed=True)
+        for tb, unroll, minb, mode in F32_PACKED:
+            s.set_config(tb, 1, unroll, 16, blocks_per_sm=minb, packed=mode)
             s.solve()
             check("f32", *s.union_rates(), u_ref, da_ref)
 
