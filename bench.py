@@ -360,6 +360,9 @@ def run_serving_leg(ctx, rate: float, duration: float, n_lo: int, n_hi: int, ste
             "queued_at_end": int(st["queued"]), "active_at_end": int(st["active"]),
             "solves_per_s": len(lat) / elapsed, "p50_latency_s": pct(0.50), "p99_latency_s": pct(0.99),
             "G_interactions_per_s_engine": st["interactions"] / max(1e-9, st["busy_seconds"]) / 1e9,
+            "engine_seconds": {"iterations": st["busy_seconds"], "admission": st["admit_seconds"],
+                               "planning": st["plan_seconds"], "retirement": st["retire_seconds"]},
+            "engine_iterations": int(st["iterations"]),
             "elapsed_s": elapsed, "arrival_replay_s": t_arrivals}
 
 

@@ -173,16 +173,22 @@ int pawan_batch_autotune(pawan_batch *batch);
 
 /* ---------------------------------------------------------------- serving */
 /* A request loop with device-resident state and continuous batching: each
- * engine iteration advances every admitted request by one RK4 step in one
- * batched launch sequence; requests that arrive meanwhile are admitted when
- * the HBM budget and the per-iteration work cap allow.  No reference
- * counterpart. */
+ * engine iteration advances every admitted request by one or more RK4 steps
+ * (as many as fit in iteration_seconds of device work without passing any
+ * active request's last step), one batched launch sequence per step (a CUDA
+ * graph per plan when it runs several); requests that
+ * arrive meanwhile are admitted when the HBM budget and the per-iteration
+ * work cap allow.  The engine takes request memory from the device's default
+ * memory pool (stream-ordered) and keeps freed memory there until it is
+ * destroyed.  No reference counterpart. */
 typedef struct {
   double budget_bytes;          /* device memory the admitted requests may hold */
   double max_step_interactions; /* cap on sum N^2 of the requests in one iteration (0: none) */
   int max_active;               /* cap on admitted requests (0: none) */
   int max_queue;                /* waiting requests beyond this are rejected (0: none) */
   int precision;                /* PAWAN_PREC_* */
+  double iteration_seconds;     /* device time one iteration may take before new arrivals
+                                   are admitted (0: 20 ms; tiny: one step per iteration) */
 } pawan_serve_config;
 
 typedef struct {
@@ -191,6 +197,9 @@ typedef struct {
   double interactions;          /* pair interactions computed (N^2 per solve per RHS) */
   double busy_seconds;          /* wall time the engine spent in iterations */
   double bytes_in_use;
+  double admit_seconds;         /* engine time creating and uploading admitted requests */
+  double plan_seconds;          /* engine time building batched plans */
+  double retire_seconds;        /* engine time copying out and releasing finished requests */
 } pawan_serve_stats;
 
 #define PAWAN_REQ_QUEUED 0

@@ -50,7 +50,7 @@ class PawanError(RuntimeError):
 class ServeConfig(ctypes.Structure):
     _fields_ = [("budget_bytes", ctypes.c_double), ("max_step_interactions", ctypes.c_double),
                 ("max_active", ctypes.c_int), ("max_queue", ctypes.c_int),
-                ("precision", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("iteration_seconds", ctypes.c_double)]
 
 
 class Tiling(ctypes.Structure):
@@ -73,7 +73,9 @@ class ServeStats(ctypes.Structure):
                 ("completed", ctypes.c_ulonglong), ("rejected", ctypes.c_ulonglong),
                 ("queued", ctypes.c_ulonglong), ("active", ctypes.c_ulonglong),
                 ("iterations", ctypes.c_ulonglong), ("interactions", ctypes.c_double),
-                ("busy_seconds", ctypes.c_double), ("bytes_in_use", ctypes.c_double)]
+                ("busy_seconds", ctypes.c_double), ("bytes_in_use", ctypes.c_double),
+                ("admit_seconds", ctypes.c_double), ("plan_seconds", ctypes.c_double),
+                ("retire_seconds", ctypes.c_double)]
 
 
 # name -> (restype, argtypes)
@@ -447,11 +449,15 @@ class Server:
     """Continuous-batching request loop (C: ``pawan_server``)."""
 
     def __init__(self, ctx: Context, budget_bytes: float, max_step_interactions: float = 0.0,
-                 max_active: int = 0, max_queue: int = 0, precision: str = "f32"):
+                 max_active: int = 0, max_queue: int = 0, precision: str = "f32",
+                 iteration_seconds: float = 0.0):
+        """iteration_seconds: device time one engine iteration may take before
+        new arrivals are admitted (0: the engine's default of 20 ms; a tiny value
+        gives one RK4 step per iteration)."""
         self.ctx = ctx
         self._lib = ctx._lib
         cfg = ServeConfig(float(budget_bytes), float(max_step_interactions), int(max_active),
-                          int(max_queue), PREC[precision])
+                          int(max_queue), PREC[precision], float(iteration_seconds))
         h = _vp()
         ctx.check(self._lib.pawan_server_create(ctx.handle, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

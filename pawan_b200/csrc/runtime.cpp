@@ -115,7 +115,8 @@ static bool tile_supported(int precision, const PairConfig &pc) {
 // system's arithmetic independent of the other systems in the plan).  Items are ordered largest first, so the dynamic
 // counter hands out the long ones early (longest-processing-time order).
 int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int precision,
-               const TileChoice &tile, std::unique_ptr<Plan> &out, int fixed_chunk_sources) {
+               const TileChoice &tile, std::unique_ptr<Plan> &out, int fixed_chunk_sources,
+               bool ordered_alloc) {
   if (systems.empty()) return fail(ctx, PAWAN_ERR_INVALID, "plan over no systems");
   if (!tile_supported(precision, tile.pc))
     return fail(ctx, PAWAN_ERR_INVALID, "unsupported pair tiling for this precision");
@@ -174,6 +175,14 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
   if (items.size() > (size_t)INT32_MAX) return fail(ctx, PAWAN_ERR_INVALID, "too many work items");
   p->n_items = (int)items.size();
 
+  if (ordered_alloc) {
+    p->partial.ordered_on(ctx->stream);
+    p->boxes.ordered_on(ctx->stream);
+    p->items.ordered_on(ctx->stream);
+    p->segs.ordered_on(ctx->stream);
+    p->stage_items.ordered_on(ctx->stream);
+    p->stage_descs.ordered_on(ctx->stream);
+  }
   PAWAN_CUDA(ctx, p->partial.alloc(partial_total));
   PAWAN_CUDA(ctx, p->boxes.alloc(box_total));
   std::vector<WorkItem> wh(items.size());
@@ -240,7 +249,9 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
   // the plan's tile boxes: repack the current states (idempotent for the
   // packed arrays, which already hold pack(X) between API calls)
   PAWAN_TRY(launch_stage_mode(ctx, *out, STAGE_PACK));
-  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  // (the host tables were staged by the copies above; an ordered plan is used
+  // on the same stream, so only the others wait here)
+  if (!ordered_alloc) PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return PAWAN_OK;
 }
 
@@ -427,6 +438,15 @@ int autotune_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, in
 int system_alloc(pawan_system *sys) {
   pawan_ctx *ctx = sys->ctx;
   const size_t n = sys->n;
+  if (sys->ordered_alloc) {
+    for (auto *b : {&sys->X, &sys->Xs, &sys->K1, &sys->K2, &sys->R, &sys->rad, &sys->vol,
+                    &sys->diag_scratch, &sys->diag_out, &sys->Xc})
+      b->ordered_on(ctx->stream);
+    sys->wake_id.ordered_on(ctx->stream);
+    for (auto *b : {&sys->pos32, &sys->vor32, &sys->poslo, &sys->vorlo}) b->ordered_on(ctx->stream);
+    sys->pos64.ordered_on(ctx->stream);
+    sys->vor64.ordered_on(ctx->stream);
+  }
   PAWAN_CUDA(ctx, sys->X.alloc(6 * n));
   PAWAN_CUDA(ctx, sys->Xs.alloc(6 * n));
   PAWAN_CUDA(ctx, sys->K1.alloc(6 * n));
@@ -450,7 +470,9 @@ int system_alloc(pawan_system *sys) {
   PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->wake_id.p, wid.data(), n * sizeof(int),
                                   cudaMemcpyHostToDevice, ctx->stream));
   PAWAN_CUDA(ctx, cudaMemsetAsync(sys->X.p, 0, 6 * n * sizeof(double), ctx->stream));
-  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  // (the pageable wake ids were staged by the copy; ordered systems are only
+  // used on this stream)
+  if (!sys->ordered_alloc) PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return PAWAN_OK;
 }
 
@@ -537,6 +559,64 @@ static void set_geometry(pawan_system *sys, const double *pos, const double *rad
   sys->oz = c[2];
   sys->r_near = std::max(4.0 * smax, 0.03 * std::sqrt(ext2));
   sys->geometry_version++;
+}
+
+static int create_system(pawan_ctx *ctx, size_t n_wakes, const size_t *num_particles, double nu,
+                         int precision, bool ordered, pawan_system **out) {
+  CHECK_CTX(ctx);
+  if (!out || n_wakes == 0 || !num_particles)
+    return fail(ctx, PAWAN_ERR_INVALID, "system needs at least one wake");
+  if (precision < PAWAN_PREC_F32 || precision > PAWAN_PREC_F64_PLAIN)
+    return fail(ctx, PAWAN_ERR_INVALID, "unknown precision");
+  if (!std::isfinite(nu) || nu < 0.0) return fail(ctx, PAWAN_ERR_INVALID, "nu must be >= 0");
+  *out = nullptr;
+  std::unique_ptr<pawan_system> sys(new pawan_system());
+  sys->ctx = ctx;
+  sys->ordered_alloc = ordered;
+  size_t off = 0;
+  for (size_t w = 0; w < n_wakes; ++w) {
+    if (num_particles[w] == 0) return fail(ctx, PAWAN_ERR_INVALID, "empty wake");
+    sys->counts.push_back(num_particles[w]);
+    sys->offsets.push_back(off);
+    off += num_particles[w];
+  }
+  if (off < 2) return fail(ctx, PAWAN_ERR_INVALID, "a system needs at least two particles");
+  if (off > (size_t)(1 << 28)) return fail(ctx, PAWAN_ERR_INVALID, "too many particles");
+  sys->n = off;
+  sys->nu = nu;
+  sys->precision = precision;
+  sys->tile = default_tile(precision);
+  PAWAN_CUDA(ctx, cudaSetDevice(ctx->device));
+  PAWAN_TRY(system_alloc(sys.get()));
+  *out = sys.release();
+  return PAWAN_OK;
+}
+
+int pawan::system_create_ordered(pawan_ctx *ctx, size_t n_wakes, const size_t *num_particles,
+                                 double nu, int precision, pawan_system **out) {
+  return create_system(ctx, n_wakes, num_particles, nu, precision, true, out);
+}
+
+int pawan::system_upload(pawan_system *sys, const double *position, const double *vorticity,
+                         const double *radius, const double *volume) {
+  CHECK_SYS(sys);
+  pawan_ctx *ctx = sys->ctx;
+  if (!position || !vorticity || !radius || !volume)
+    return fail(ctx, PAWAN_ERR_INVALID, "null particle array");
+  const size_t N = sys->n;
+  for (size_t i = 0; i < N; ++i)
+    if (!(radius[i] > 0.0) || !std::isfinite(radius[i]))
+      return fail(ctx, PAWAN_ERR_INVALID, "smoothing radii must be positive");
+  for (size_t i = 0; i < 3 * N; ++i)
+    if (!std::isfinite(position[i]) || !std::isfinite(vorticity[i]))
+      return fail(ctx, PAWAN_ERR_INVALID, "non-finite position or vorticity");
+  set_geometry(sys, position, radius);
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->X.p, position, 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->X.p + 3 * N, vorticity, 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->rad.p, radius, N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->vol.p, volume, N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  sys->has_particles = true;
+  return PAWAN_OK;
 }
 
 extern "C" {
@@ -701,36 +781,13 @@ int pawan_host_free(pawan_ctx *ctx, void *ptr) {
 
 int pawan_system_create(pawan_ctx *ctx, size_t n_wakes, const size_t *num_particles, double nu,
                         int precision, pawan_system **out) {
-  CHECK_CTX(ctx);
-  if (!out || n_wakes == 0 || !num_particles)
-    return fail(ctx, PAWAN_ERR_INVALID, "system needs at least one wake");
-  if (precision < PAWAN_PREC_F32 || precision > PAWAN_PREC_F64_PLAIN)
-    return fail(ctx, PAWAN_ERR_INVALID, "unknown precision");
-  if (!std::isfinite(nu) || nu < 0.0) return fail(ctx, PAWAN_ERR_INVALID, "nu must be >= 0");
-  *out = nullptr;
-  std::unique_ptr<pawan_system> sys(new pawan_system());
-  sys->ctx = ctx;
-  size_t off = 0;
-  for (size_t w = 0; w < n_wakes; ++w) {
-    if (num_particles[w] == 0) return fail(ctx, PAWAN_ERR_INVALID, "empty wake");
-    sys->counts.push_back(num_particles[w]);
-    sys->offsets.push_back(off);
-    off += num_particles[w];
-  }
-  if (off < 2) return fail(ctx, PAWAN_ERR_INVALID, "a system needs at least two particles");
-  if (off > (size_t)(1 << 28)) return fail(ctx, PAWAN_ERR_INVALID, "too many particles");
-  sys->n = off;
-  sys->nu = nu;
-  sys->precision = precision;
-  sys->tile = default_tile(precision);
-  PAWAN_CUDA(ctx, cudaSetDevice(ctx->device));
-  PAWAN_TRY(system_alloc(sys.get()));
-  *out = sys.release();
-  return PAWAN_OK;
+  return create_system(ctx, n_wakes, num_particles, nu, precision, false, out);
 }
 
 // Device buffers are released with cudaFree, which waits for outstanding
-// work on them; the context is not touched, so a system may outlive it.
+// work on them; the context is not touched, so a system may outlive it
+// (except one created by the serving engine, whose buffers go back to the
+// memory pool on the context's stream).
 void pawan_system_destroy(pawan_system *sys) {
   if (!sys) return;
   delete sys;
@@ -741,25 +798,9 @@ size_t pawan_system_num_particles(const pawan_system *sys) { return sys ? sys->n
 
 int pawan_system_set_particles(pawan_system *sys, const double *position, const double *vorticity,
                                const double *radius, const double *volume) {
-  CHECK_SYS(sys);
-  pawan_ctx *ctx = sys->ctx;
-  if (!position || !vorticity || !radius || !volume)
-    return fail(ctx, PAWAN_ERR_INVALID, "null particle array");
-  const size_t N = sys->n;
-  for (size_t i = 0; i < N; ++i)
-    if (!(radius[i] > 0.0) || !std::isfinite(radius[i]))
-      return fail(ctx, PAWAN_ERR_INVALID, "smoothing radii must be positive");
-  for (size_t i = 0; i < 3 * N; ++i)
-    if (!std::isfinite(position[i]) || !std::isfinite(vorticity[i]))
-      return fail(ctx, PAWAN_ERR_INVALID, "non-finite position or vorticity");
-  set_geometry(sys, position, radius);
-  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->X.p, position, 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->X.p + 3 * N, vorticity, 3 * N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->rad.p, radius, N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  PAWAN_CUDA(ctx, cudaMemcpyAsync(sys->vol.p, volume, N * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  sys->has_particles = true;
+  PAWAN_TRY(system_upload(sys, position, vorticity, radius, volume));
   PAWAN_TRY(pack_after_state(sys));
-  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  PAWAN_CUDA(sys->ctx, cudaStreamSynchronize(sys->ctx->stream));
   return PAWAN_OK;
 }
 

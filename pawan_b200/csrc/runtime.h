@@ -17,19 +17,30 @@
 
 namespace pawan {
 
-// A device allocation that frees itself.
+// A device allocation that frees itself.  By default cudaMalloc / cudaFree
+// (the free waits for the device); after ordered_on(stream) the buffer is
+// taken from and returned to the device's memory pool in the order of
+// `stream` (cudaMallocAsync / cudaFreeAsync, no device-wide synchronisation),
+// so every use must be ordered on that stream before the buffer is released.
 template <class T>
 struct DBuf {
   T *p = nullptr;
   size_t n = 0;
+  cudaStream_t stream = nullptr;
+  bool ordered = false;
   DBuf() = default;
   DBuf(const DBuf &) = delete;
   DBuf &operator=(const DBuf &) = delete;
   ~DBuf() { reset(); }
+  void ordered_on(cudaStream_t s) {
+    stream = s;
+    ordered = true;
+  }
   cudaError_t alloc(size_t count) {
     reset();
     if (count == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&p), count * sizeof(T));
+    cudaError_t e = ordered ? cudaMallocAsync(reinterpret_cast<void **>(&p), count * sizeof(T), stream)
+                            : cudaMalloc(reinterpret_cast<void **>(&p), count * sizeof(T));
     if (e != cudaSuccess) {
       p = nullptr;
       return e;
@@ -38,7 +49,12 @@ struct DBuf {
     return cudaSuccess;
   }
   void reset() {
-    if (p) cudaFree(p);
+    if (p) {
+      if (ordered)
+        cudaFreeAsync(p, stream);
+      else
+        cudaFree(p);
+    }
     p = nullptr;
     n = 0;
   }
@@ -106,6 +122,9 @@ struct pawan_system {
   double r_near = 0;
   unsigned long long geometry_version = 0;  // bumps when origin / r_near change
   unsigned long long pack_version = 0;      // bumps whenever the packed arrays change
+  // device buffers from the memory pool in the order of ctx->stream (systems
+  // owned by the serving engine); the context must outlive the system
+  bool ordered_alloc = false;
   size_t device_bytes() const;
 };
 
@@ -145,7 +164,8 @@ int fail(pawan_ctx *ctx, int code, const std::string &msg);
 int cuda_fail(pawan_ctx *ctx, cudaError_t e, const char *where);
 
 int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int precision,
-               const TileChoice &tile, std::unique_ptr<Plan> &out, int fixed_chunk_sources = 0);
+               const TileChoice &tile, std::unique_ptr<Plan> &out, int fixed_chunk_sources = 0,
+               bool ordered_alloc = false);
 int set_plan_dt(pawan_ctx *ctx, Plan &p, const double *dt, double dt0);
 int launch_pairs(pawan_ctx *ctx, Plan &p, bool allow_events = true);
 int launch_stage_mode(pawan_ctx *ctx, Plan &p, int mode);
@@ -153,6 +173,14 @@ int rk4_steps(pawan_ctx *ctx, Plan &p, size_t nsteps, bool use_graph);
 int autotune_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int precision,
                   TileChoice *best);
 int system_alloc(pawan_system *sys);
+// A system without device-side plan (the serving engine plans over many):
+// creation with buffers from the memory pool (ordered on ctx->stream), and
+// the particle upload (validation, geometry, copies; packing is left to the
+// next plan built over the system).  Neither waits for the device.
+int system_create_ordered(pawan_ctx *ctx, size_t n_wakes, const size_t *num_particles, double nu,
+                          int precision, pawan_system **out);
+int system_upload(pawan_system *sys, const double *position, const double *vorticity,
+                  const double *radius, const double *volume);
 int system_ensure_plan(pawan_system *sys);
 int state_to_device(pawan_system *sys, const double *state);
 int state_from_device(pawan_system *sys, const double *dev_union, double *state);

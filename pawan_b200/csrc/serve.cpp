@@ -5,10 +5,23 @@
 // and step count.  The worker thread repeats: admit waiting requests in
 // arrival order while the device-memory budget, the active-request cap and the
 // per-iteration work cap (sum N^2) allow; advance every admitted request by
-// one RK4 step in one batched launch sequence (one persistent pair launch per
-// stage over all of them); retire the finished ones (state copied to the
-// host, device memory released).  Requests that arrive while others run join
-// at the next iteration, so their work overlaps on the device.
+// k RK4 steps in one batched launch sequence per step (one persistent pair
+// launch per stage over all of them); retire the finished ones (state copied
+// to the host, device memory released).  Requests that arrive while others
+// run join at the next iteration, so their work overlaps on the device.
+//
+// k is the largest step count that neither runs past the first active
+// request's last step nor makes the iteration longer than the configured
+// target (kIterTarget by default) at the device rate measured so far, so a
+// new arrival waits at most
+// about that long for admission while few or small active requests do not
+// pay one host round trip per step.
+//
+// The engine's systems and plans take their device memory from the device's
+// memory pool in the order of the engine's stream (cudaMallocAsync /
+// cudaFreeAsync): admitting and retiring requests never synchronises the
+// device, and a request's particles are packed by the batched plan built
+// after its admission instead of a plan of its own.
 //
 // Sources are chunked in fixed-size chunks per request, so a request's
 // arithmetic does not depend on which other requests share its launches: its
@@ -21,6 +34,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdint>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -34,6 +48,8 @@ using namespace pawan;
 namespace {
 
 constexpr int kServeChunkSources = 8192;
+constexpr double kIterTarget = 0.02;     // default seconds of device work per iteration
+constexpr double kRateGuess = 3e11;      // interactions/s before the first measurement
 
 double now_since(std::chrono::steady_clock::time_point t0) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
@@ -81,6 +97,8 @@ struct pawan_server {
   double bytes_in_use = 0.0;
   std::string worker_error;
   TileChoice tile;
+  double rate = kRateGuess;  // measured interactions/s of the iterations (worker only)
+  cudaMemPool_t pool = nullptr;
 };
 
 namespace {
@@ -90,26 +108,47 @@ void finish(pawan_server *srv, Request *r, int state) {
   r->t_done = now_since(srv->t0);
 }
 
-// One engine iteration on the admitted requests; called without the lock.
-int run_iteration(pawan_server *srv, std::vector<Request *> &act, std::unique_ptr<Plan> &plan,
-                  bool rebuild) {
+// Builds the batched plan over the admitted requests (when the set changed);
+// called without the lock.
+int plan_iteration(pawan_server *srv, std::vector<Request *> &act, std::unique_ptr<Plan> &plan,
+                   bool rebuild) {
   pawan_ctx *ctx = srv->ctx;
   if (rebuild || !plan) {
     plan.reset();
     std::vector<pawan_system *> sys;
     for (Request *r : act) sys.push_back(r->sys);
-    int st = build_plan(ctx, sys, srv->cfg.precision, srv->tile, plan, kServeChunkSources);
+    int st = build_plan(ctx, sys, srv->cfg.precision, srv->tile, plan, kServeChunkSources, true);
     if (st != PAWAN_OK) return st;
   }
   std::vector<double> dts;
   for (Request *r : act) dts.push_back(r->dt);
-  int st = set_plan_dt(ctx, *plan, dts.data(), 0.0);
-  if (st != PAWAN_OK) return st;
-  st = rk4_steps(ctx, *plan, 1, false);
+  return set_plan_dt(ctx, *plan, dts.data(), 0.0);
+}
+
+// k RK4 steps of every admitted request (replays of the plan's captured step
+// when there are several), then waits for the device.
+int run_iteration(pawan_server *srv, Plan &plan, size_t k) {
+  pawan_ctx *ctx = srv->ctx;
+  int st = rk4_steps(ctx, plan, k, k >= 3);
   if (st != PAWAN_OK) return st;
   cudaError_t e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "serving iteration");
   return PAWAN_OK;
+}
+
+// Steps per iteration (see the file comment).
+size_t steps_per_iteration(const pawan_server *srv, const std::vector<Request *> &act) {
+  size_t min_left = ~(size_t)0;
+  double n2 = 0.0;
+  for (const Request *r : act) {
+    min_left = std::min(min_left, r->nsteps - r->steps_done);
+    n2 += (double)r->n * (double)r->n;
+  }
+  const double step_s = 4.0 * n2 / std::max(1e9, srv->rate);
+  const double target = srv->cfg.iteration_seconds > 0.0 ? srv->cfg.iteration_seconds : kIterTarget;
+  const double fit = std::floor(target / std::max(1e-9, step_s));
+  const size_t k = fit < 1.0 ? 1 : (fit > 1e6 ? (size_t)1000000 : (size_t)fit);
+  return std::max<size_t>(1, std::min(k, min_left));
 }
 
 void worker_main(pawan_server *srv) {
@@ -147,12 +186,12 @@ void worker_main(pawan_server *srv) {
       if (srv->stop && admit.empty() && srv->active.empty()) break;
     }
     // create device state of newly admitted requests (outside the lock)
+    const auto ta0 = std::chrono::steady_clock::now();
     for (Request *r : admit) {
-      int st = pawan_system_create(srv->ctx, r->counts.size(), r->counts.data(), r->nu,
-                                   srv->cfg.precision, &r->sys);
+      int st = system_create_ordered(srv->ctx, r->counts.size(), r->counts.data(), r->nu,
+                                     srv->cfg.precision, &r->sys);
       if (st == PAWAN_OK)
-        st = pawan_system_set_particles(r->sys, r->pos.data(), r->vor.data(), r->rad.data(),
-                                        r->vol.data());
+        st = system_upload(r->sys, r->pos.data(), r->vor.data(), r->rad.data(), r->vol.data());
       std::lock_guard<std::mutex> lk(srv->mu);
       if (st != PAWAN_OK) {
         srv->worker_error = srv->ctx->err;
@@ -164,11 +203,17 @@ void worker_main(pawan_server *srv) {
         srv->cv_done.notify_all();
         continue;
       }
+      // (the pageable particle copies were staged before system_upload returned)
       std::vector<double>().swap(r->pos);
       std::vector<double>().swap(r->vor);
       srv->active.push_back(r);
       srv->stats.admitted++;
       set_changed = true;
+    }
+    if (!admit.empty()) {
+      std::lock_guard<std::mutex> lk(srv->mu);
+      srv->stats.admit_seconds +=
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - ta0).count();
     }
     std::vector<Request *> act;
     {
@@ -176,25 +221,41 @@ void worker_main(pawan_server *srv) {
       act = srv->active;
     }
     if (act.empty()) continue;
-    const auto it0 = std::chrono::steady_clock::now();
-    int st = run_iteration(srv, act, plan, set_changed);
+    const auto tp0 = std::chrono::steady_clock::now();
+    int st = plan_iteration(srv, act, plan, set_changed);
     set_changed = false;
-    const double busy = std::chrono::duration<double>(std::chrono::steady_clock::now() - it0).count();
+    const auto it0 = std::chrono::steady_clock::now();
+    size_t k = 0;
+    double n2 = 0.0;
+    for (Request *r : act) n2 += (double)r->n * (double)r->n;
+    if (st == PAWAN_OK) {
+      k = steps_per_iteration(srv, act);
+      st = run_iteration(srv, *plan, k);
+    }
+    const auto it1 = std::chrono::steady_clock::now();
+    const double busy = std::chrono::duration<double>(it1 - it0).count();
+    if (st == PAWAN_OK && busy > 0.0) {
+      // device rate of this iteration, smoothed (for the next step count)
+      const double r = 4.0 * n2 * (double)k / busy;
+      srv->rate = 0.5 * srv->rate + 0.5 * r;
+    }
     // retire finished / cancelled requests
     std::vector<Request *> done;
     {
       std::lock_guard<std::mutex> lk(srv->mu);
       srv->stats.iterations++;
       srv->stats.busy_seconds += busy;
+      srv->stats.plan_seconds += std::chrono::duration<double>(it0 - tp0).count();
       if (st != PAWAN_OK) srv->worker_error = srv->ctx->err;
       for (Request *r : act) {
         if (st == PAWAN_OK) {
-          r->steps_done++;
-          srv->stats.interactions += 4.0 * (double)r->n * (double)r->n;
+          r->steps_done += k;
+          srv->stats.interactions += 4.0 * (double)r->n * (double)r->n * (double)k;
         }
         if (st != PAWAN_OK || r->cancel || r->steps_done >= r->nsteps) done.push_back(r);
       }
     }
+    const auto tr0 = std::chrono::steady_clock::now();
     for (Request *r : done) {
       int state = PAWAN_REQ_DONE;
       if (st != PAWAN_OK) {
@@ -218,10 +279,13 @@ void worker_main(pawan_server *srv) {
     }
     if (!done.empty()) {
       std::lock_guard<std::mutex> lk(srv->mu);
+      srv->stats.retire_seconds +=
+          std::chrono::duration<double>(std::chrono::steady_clock::now() - tr0).count();
       srv->cv_done.notify_all();
     }
   }
   plan.reset();
+  cudaStreamSynchronize(srv->ctx->stream);  // the plan's buffers are back in the pool
 }
 
 }  // namespace
@@ -231,13 +295,21 @@ extern "C" {
 int pawan_server_create(pawan_ctx *ctx, const pawan_serve_config *cfg, pawan_server **out) {
   if (!ctx || !cfg || !out) return PAWAN_ERR_INVALID;
   if (!(cfg->budget_bytes > 0) || cfg->precision < PAWAN_PREC_F32 ||
-      cfg->precision > PAWAN_PREC_F64_PLAIN)
+      cfg->precision > PAWAN_PREC_F64_PLAIN || !(cfg->iteration_seconds >= 0.0))
     return fail(ctx, PAWAN_ERR_INVALID, "bad serving configuration");
   std::unique_ptr<pawan_server> srv(new pawan_server());
   srv->cfg = *cfg;
   srv->tile = default_tile(cfg->precision);
   int st = pawan_ctx_create(ctx->device, &srv->ctx);
   if (st != PAWAN_OK) return fail(ctx, st, "cannot create the serving context");
+  // freed request memory stays in the device's pool for the next admission
+  // (it goes back to the system when the engine is destroyed)
+  if (cudaDeviceGetDefaultMemPool(&srv->pool, srv->ctx->device) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(srv->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  } else {
+    srv->pool = nullptr;
+  }
   srv->t0 = std::chrono::steady_clock::now();
   pawan_server *raw = srv.get();
   try {
@@ -264,6 +336,8 @@ void pawan_server_destroy(pawan_server *srv) {
   if (srv->worker.joinable()) srv->worker.join();
   for (auto &kv : srv->reqs)
     if (kv.second->sys) pawan_system_destroy(kv.second->sys);
+  cudaStreamSynchronize(srv->ctx->stream);
+  if (srv->pool) cudaMemPoolTrimTo(srv->pool, 0);
   pawan_ctx_destroy(srv->ctx);
   delete srv;
 }

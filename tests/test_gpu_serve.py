@@ -30,7 +30,8 @@ def run_alone(ctx, sc):
 
 def test_alone_and_in_the_mix_are_identical(ctx):
     scs = requests()
-    srv = Server(ctx, budget_bytes=1 << 30)
+    # one RK4 step per iteration, so the staggered arrivals join requests in flight
+    srv = Server(ctx, budget_bytes=1 << 30, iteration_seconds=1e-9)
     ids = []
     for k, sc in enumerate(scs):
         st, rid = srv.submit_scenario(sc)
@@ -51,6 +52,34 @@ def test_alone_and_in_the_mix_are_identical(ctx):
         solo.rk4(sc.dt, sc.steps)
         st0 = sc.state()
         assert rms_rel(out - st0, solo.get_states() - st0) < 1e-12
+    # at least one request was admitted while another was still running
+    spans = [(ta, td) for _, ts, ta, td in mixed]
+    assert any(a2 < d1 and a1 <= a2 for i, (a1, d1) in enumerate(spans)
+               for j, (a2, d2) in enumerate(spans) if i != j)
+
+
+def test_multi_step_iterations_match_single_steps(ctx):
+    """The default policy runs several RK4 steps per iteration (CUDA-graph
+    replays); every request's result is bit-identical to one step per
+    iteration, and all requests finish."""
+    reqs = g.serving_requests(rate=1000.0, duration=1.0, seed=9, n_lo=64, n_hi=1500,
+                              steps_lo=10, steps_hi=40)
+    scs = [r.scenario for r in reqs[:8]]
+    outs = []
+    for target in (0.0, 1e-9):
+        srv = Server(ctx, budget_bytes=1 << 30, iteration_seconds=target)
+        ids = [srv.submit_scenario(sc)[1] for sc in scs]
+        for rid in ids:
+            assert srv.wait(rid, 120)
+        outs.append([srv.fetch(rid)[0] for rid in ids])
+        stats = srv.stats()
+        srv.close()
+        assert stats["completed"] == len(scs)
+        if target == 0.0:
+            # fewer iterations than the longest request has steps
+            assert stats["iterations"] < max(sc.steps for sc in scs)
+    for a, b in zip(*outs):
+        assert a is not None and np.array_equal(a, b)
 
 
 def test_budget_rejects_oversized_request(ctx):
@@ -66,7 +95,7 @@ def test_budget_serialises_admission(ctx):
     """A budget that fits one request at a time: all finish, never two active."""
     scs = [g.single_ring(n_stations=128, seed=s, steps=3) for s in (1, 2, 3)]
     probe = Server(ctx, budget_bytes=1 << 30)
-    rid = probe.submit_scenario(scs[0], nsteps=400)[1]
+    rid = probe.submit_scenario(scs[0], nsteps=10_000_000)[1]  # cancelled below
     while probe.poll(rid) == "queued":
         time.sleep(0.001)
     one = probe.stats()["bytes_in_use"]
