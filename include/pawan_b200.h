@@ -133,6 +133,12 @@ int pawan_system_euler(pawan_system *sys, double dt, size_t nsteps);
 int pawan_system_diagnose(pawan_system *sys, double *out, int quadratic);
 /* calculateKineticEnergy over all wakes (interaction.cpp:351-383). */
 int pawan_system_kinetic_energy(pawan_system *sys, double *ke);
+/* __interaction::resolve -> influence (interaction.cpp:45-47, 110-155): the
+ * smoothed vorticity field of every particle, FP64 on the device, into
+ * `field` (3N doubles, the wakes' _vorticityfield rows in wake order).  The
+ * influence-matrix path of __resolve::rebuild (src/resolve/resolve.cpp:10-57)
+ * calls it once per state component. */
+int pawan_system_influence(pawan_system *sys, double *field, size_t size);
 /* The protected __interaction::_nu (interaction.h:24). */
 int pawan_system_set_nu(pawan_system *sys, double nu);
 int pawan_system_set_precision(pawan_system *sys, int precision);

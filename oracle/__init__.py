@@ -71,6 +71,13 @@ def _load_ref():
         lib.refh_kinetic_energy.argtypes = [ctypes.c_void_p]
         lib.refh_write_frame.restype = ctypes.c_int
         lib.refh_write_frame.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_double, ctypes.c_int]
+        lib.refh_vring_create.restype = ctypes.c_void_p
+        lib.refh_vring_create.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double]
+        lib.refh_num_particles.restype = ctypes.c_size_t
+        lib.refh_num_particles.argtypes = [ctypes.c_void_p]
+        lib.refh_get_particles.argtypes = [ctypes.c_void_p, _dp, _dp, _dp, _dp]
+        lib.refh_influence.argtypes = [ctypes.c_void_p, _dp]
+        lib.refh_resolve.argtypes = [ctypes.c_void_p, _dp]
         lib.refh_set_threads.argtypes = [ctypes.c_int]
         lib.refh_max_threads.restype = ctypes.c_int
         lib.refh_wtime.restype = ctypes.c_double
@@ -91,6 +98,7 @@ def _load_orc():
         for name in ("orc_enstrophy", "orc_helicity"):
             getattr(lib, name).restype = ctypes.c_double
             getattr(lib, name).argtypes = [ctypes.c_size_t, _dp, _dp, _dp]
+        lib.orc_influence.argtypes = [ctypes.c_size_t, _dp, _dp, _dp, _dp]
         lib.orc_kinetic_energy.restype = ctypes.c_double
         lib.orc_kinetic_energy.argtypes = [ctypes.c_size_t, _i32p, _dp, _dp, _dp]
         _orc = lib
@@ -180,6 +188,40 @@ class RefSystem:
         if self._lib.refh_write_frame(self._h, path.encode(), float(t), 1 if append else 0) != 0:
             raise OSError(f"cannot open {path}")
 
+    def influence(self) -> np.ndarray:
+        """__interaction::resolve() -> influence(): the vorticity field (N x 3)."""
+        k = np.empty((self._lib.refh_num_particles(self._h), 3))
+        self._lib.refh_influence(self._h, _ptr(k))
+        return k
+
+    def particles(self):
+        """(pos, vor, rad, vol) of the wakes, union order."""
+        n = self._lib.refh_num_particles(self._h)
+        pos, vor, rad, vol = np.empty((n, 3)), np.empty((n, 3)), np.empty(n), np.empty(n)
+        self._lib.refh_get_particles(self._h, _ptr(pos), _ptr(vor), _ptr(rad), _ptr(vol))
+        return pos, vor, rad, vol
+
+    def resolve(self) -> np.ndarray:
+        """__resolve::rebuild on this system (writes data/temp.wakeinfluence in
+        the current directory); returns the resolved state."""
+        s = np.empty(self.size)
+        self._lib.refh_resolve(self._h, _ptr(s))
+        return s
+
+
+class RefVring(RefSystem):
+    """The reference's ``__vring(radius, core, layers)`` (src/wake/vring.cpp:51-104)
+    in a serial ``__interaction``; its state is the per-layer strength vector."""
+
+    def __init__(self, radius: float, core: float, layers: int, nu: float = 0.0):
+        lib = _load_ref()
+        self._lib = lib
+        self._h = lib.refh_vring_create(float(radius), float(core), int(layers), float(nu))
+        self.n = lib.refh_num_particles(self._h)
+        self.counts = [self.n]
+        self.parallel = False
+        self.size = lib.refh_size(self._h)
+
 
 def ref_set_threads(n: int):
     _load_ref().refh_set_threads(int(n))
@@ -235,6 +277,14 @@ def enstrophy(pos, vor, rad) -> float:
 def helicity(pos, vor, rad) -> float:
     pos, vor, rad = _f64(pos), _f64(vor), _f64(rad)
     return float(_load_orc().orc_helicity(rad.shape[0], _ptr(pos), _ptr(vor), _ptr(rad)))
+
+
+def influence(pos, vor, rad) -> np.ndarray:
+    """Vorticity field K_i = Z(0, s_i) alpha_i + sum_j Z_ij alpha_j (N x 3), FP64."""
+    pos, vor, rad = _f64(pos), _f64(vor), _f64(rad)
+    k = np.empty((rad.shape[0], 3))
+    _load_orc().orc_influence(rad.shape[0], _ptr(pos), _ptr(vor), _ptr(rad), _ptr(k))
+    return k
 
 
 def kinetic_energy(wake_id, pos, vor, rad) -> float:

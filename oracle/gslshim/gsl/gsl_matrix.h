@@ -19,6 +19,7 @@ void gsl_matrix_set_zero(gsl_matrix *m);
 int gsl_matrix_memcpy(gsl_matrix *dest, const gsl_matrix *src);
 
 gsl_vector_view gsl_matrix_row(gsl_matrix *m, size_t i);
+gsl_vector_view gsl_matrix_column(gsl_matrix *m, size_t j);
 gsl_vector_const_view gsl_matrix_const_row(const gsl_matrix *m, size_t i);
 gsl_matrix_view gsl_matrix_view_vector(gsl_vector *v, size_t n1, size_t n2);
 gsl_matrix_const_view gsl_matrix_const_view_vector(const gsl_vector *v, size_t n1, size_t n2);

@@ -8,8 +8,10 @@
 #include <string.h>
 
 #include "gsl/gsl_blas.h"
+#include "gsl/gsl_linalg.h"
 #include "gsl/gsl_math.h"
 #include "gsl/gsl_matrix.h"
+#include "gsl/gsl_permutation.h"
 #include "gsl/gsl_vector.h"
 
 void gslshim_fail(const char *what, const char *file, int line) {
@@ -240,6 +242,17 @@ gsl_vector_view gsl_matrix_row(gsl_matrix *m, size_t i) {
   return view;
 }
 
+gsl_vector_view gsl_matrix_column(gsl_matrix *m, size_t j) {
+  SHIM_REQUIRE(j < m->size2, "matrix column out of range");
+  gsl_vector_view view;
+  view.vector.size = m->size1;
+  view.vector.stride = m->tda;
+  view.vector.data = m->data + j;
+  view.vector.block = m->block;
+  view.vector.owner = 0;
+  return view;
+}
+
 gsl_vector_const_view gsl_matrix_const_row(const gsl_matrix *m, size_t i) {
   SHIM_REQUIRE(i < m->size1, "matrix row out of range");
   _gsl_vector_const_view view;
@@ -359,4 +372,101 @@ double gsl_pow_7(const double x) {
 double gsl_hypot(const double x, const double y) { return hypot(x, y); }
 double gsl_hypot3(const double x, const double y, const double z) {
   return sqrt(x * x + y * y + z * z);
+}
+
+/* ----------------------------------------------------------- permutations */
+
+gsl_permutation *gsl_permutation_alloc(size_t n) {
+  gsl_permutation *p = (gsl_permutation *)malloc(sizeof(gsl_permutation));
+  SHIM_REQUIRE(p != NULL, "permutation allocation failed");
+  p->data = (size_t *)malloc((n ? n : 1) * sizeof(size_t));
+  SHIM_REQUIRE(p->data != NULL, "permutation data allocation failed");
+  p->size = n;
+  return p;
+}
+
+gsl_permutation *gsl_permutation_calloc(size_t n) {
+  gsl_permutation *p = gsl_permutation_alloc(n);
+  gsl_permutation_init(p);
+  return p;
+}
+
+void gsl_permutation_init(gsl_permutation *p) {
+  for (size_t i = 0; i < p->size; ++i) p->data[i] = i;
+}
+
+void gsl_permutation_free(gsl_permutation *p) {
+  if (!p) return;
+  free(p->data);
+  free(p);
+}
+
+size_t gsl_permutation_get(const gsl_permutation *p, size_t i) {
+  SHIM_REQUIRE(i < p->size, "permutation index out of range");
+  return p->data[i];
+}
+
+/* ------------------------------------------------------------------- LU */
+
+/* Gaussian elimination with partial pivoting (row interchanges), column by
+ * column: the pivot of column j is the largest |a_ij| on or below the
+ * diagonal; rows are swapped in place and the swap recorded in p. */
+int gsl_linalg_LU_decomp(gsl_matrix *A, gsl_permutation *p, int *signum) {
+  SHIM_REQUIRE(A->size1 == A->size2, "LU of a non-square matrix");
+  SHIM_REQUIRE(p->size == A->size1, "permutation length != matrix size");
+  const size_t n = A->size1, t = A->tda;
+  double *a = A->data;
+  gsl_permutation_init(p);
+  *signum = 1;
+  for (size_t j = 0; j + 1 < n; ++j) {
+    size_t piv = j;
+    double best = fabs(a[j * t + j]);
+    for (size_t i = j + 1; i < n; ++i) {
+      const double v = fabs(a[i * t + j]);
+      if (v > best) {
+        best = v;
+        piv = i;
+      }
+    }
+    if (piv != j) {
+      for (size_t k = 0; k < n; ++k) {
+        const double tmp = a[j * t + k];
+        a[j * t + k] = a[piv * t + k];
+        a[piv * t + k] = tmp;
+      }
+      const size_t tp = p->data[j];
+      p->data[j] = p->data[piv];
+      p->data[piv] = tp;
+      *signum = -*signum;
+    }
+    const double ajj = a[j * t + j];
+    if (ajj != 0.0) {
+      for (size_t i = j + 1; i < n; ++i) {
+        const double lij = a[i * t + j] / ajj;
+        a[i * t + j] = lij;
+        for (size_t k = j + 1; k < n; ++k) a[i * t + k] -= lij * a[j * t + k];
+      }
+    }
+  }
+  return GSL_SUCCESS;
+}
+
+int gsl_linalg_LU_solve(const gsl_matrix *LU, const gsl_permutation *p, const gsl_vector *b,
+                        gsl_vector *x) {
+  SHIM_REQUIRE(LU->size1 == LU->size2, "LU of a non-square matrix");
+  const size_t n = LU->size1, t = LU->tda;
+  SHIM_REQUIRE(p->size == n && b->size == n && x->size == n, "LU solve size mismatch");
+  const double *a = LU->data;
+  double *y = (double *)malloc((n ? n : 1) * sizeof(double));
+  SHIM_REQUIRE(y != NULL, "LU solve allocation failed");
+  for (size_t i = 0; i < n; ++i) y[i] = b->data[p->data[i] * b->stride];
+  for (size_t i = 0; i < n; ++i) /* L y = P b, unit diagonal */
+    for (size_t k = 0; k < i; ++k) y[i] -= a[i * t + k] * y[k];
+  for (size_t ii = n; ii-- > 0;) { /* U x = y */
+    for (size_t k = ii + 1; k < n; ++k) y[ii] -= a[ii * t + k] * y[k];
+    y[ii] /= a[ii * t + ii];
+  }
+  for (size_t i = 0; i < n; ++i) x->data[i * x->stride] = y[i];
+  free(y);
+  return GSL_SUCCESS;
 }

@@ -20,6 +20,12 @@
 //   refh_kinetic_energy    calculateKineticEnergy (interaction.cpp:351-383)
 //   refh_write_frame       one .wake frame: t, then __interaction::write
 //                          (interaction.cpp:197-202, wake.cpp:68-73)
+//   refh_vring_create      a __vring(R, core, layers) (src/wake/vring.cpp:51-104)
+//                          in a serial __interaction
+//   refh_influence         __interaction::resolve -> influence (interaction.cpp:45-47,
+//                          110-155): every wake's _vorticityfield
+//   refh_resolve           __resolve::rebuild (src/resolve/resolve.cpp:10-57), which
+//                          writes data/temp.wakeinfluence under the current directory
 #include <omp.h>
 
 #include <cstdio>
@@ -31,6 +37,8 @@
 #include "src/interaction/interaction.h"
 #include "src/interaction/parallel.h"
 #include "src/io/io.h"
+#include "src/resolve/resolve.h"
+#include "src/wake/vring.h"
 #include "src/wake/wake.h"
 
 namespace {
@@ -220,6 +228,59 @@ int refh_write_frame(void *p, const char *path, double t, int append) {
   h->sys()->write(f);
   std::fclose(f);
   return 0;
+}
+
+void *refh_vring_create(double radius, double core, int layers, double nu) {
+  Handle *h = new Handle();
+  h->wakes.push_back(new pawan::__vring(radius, core, layers));
+  h->serial = new SerialSystem(nu);
+  h->serial->addWake(h->wakes[0]);
+  return h;
+}
+
+size_t refh_num_particles(void *p) {
+  size_t n = 0;
+  for (auto *w : static_cast<Handle *>(p)->wakes) n += w->_numParticles;
+  return n;
+}
+
+// Union (wake order) of positions, vorticities (N x 3), radii and volumes.
+void refh_get_particles(void *p, double *pos, double *vor, double *rad, double *vol) {
+  size_t o = 0;
+  for (auto *W : static_cast<Handle *>(p)->wakes) {
+    for (size_t i = 0; i < W->_numParticles; ++i) {
+      for (size_t d = 0; d < 3; ++d) {
+        pos[3 * (o + i) + d] = gsl_matrix_get(W->_position, i, d);
+        vor[3 * (o + i) + d] = gsl_matrix_get(W->_vorticity, i, d);
+      }
+      rad[o + i] = gsl_vector_get(W->_radius, i);
+      vol[o + i] = gsl_vector_get(W->_volume, i);
+    }
+    o += W->_numParticles;
+  }
+}
+
+// __interaction::resolve() (the vorticity field), then every wake's
+// _vorticityfield in wake order (N x 3).
+void refh_influence(void *p, double *field) {
+  Handle *h = static_cast<Handle *>(p);
+  h->sys()->resolve();
+  size_t o = 0;
+  for (auto *W : h->wakes) {
+    for (size_t i = 0; i < W->_numParticles; ++i)
+      for (size_t d = 0; d < 3; ++d) field[3 * (o + i) + d] = gsl_matrix_get(W->_vorticityfield, i, d);
+    o += W->_numParticles;
+  }
+}
+
+// __resolve::rebuild(IN, IO), then the system's state (length _size).
+void refh_resolve(void *p, double *state) {
+  Handle *h = static_cast<Handle *>(p);
+  pawan::__io io;
+  pawan::__resolve rs;
+  rs.rebuild(h->sys(), &io);
+  gsl_vector_view v = gsl_vector_view_array(state, h->sys()->_size);
+  h->sys()->getStates(&v.vector);
 }
 
 void refh_set_threads(int n) { omp_set_num_threads(n); }

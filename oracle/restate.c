@@ -226,3 +226,32 @@ double orc_kinetic_energy(size_t n, const int32_t *wake_id, const double *pos,
   }
   return total;
 }
+
+/* Vorticity field, __interaction::influence (interaction.cpp:110-155):
+ *   SELFINFLUENCE (interaction_utils.h:593-605): K_i += ZETASIG(0, s_i) alpha_i
+ *   INFLUENCE (:519-556): sigma = sqrt(0.5 (s_i^2 + s_j^2)), rho = |x_i - x_j|,
+ *     Z = ZETASIG(rho, sigma) (highorder.h:20-23); K_target += Z alpha_source and
+ *     K_source += Z alpha_target (VORTICITY :38-43), i.e. in gather form
+ *     K_i += Z alpha_j for every j != i. */
+void orc_influence(size_t n, const double *pos, const double *vor, const double *rad,
+                   double *field) {
+#pragma omp parallel for schedule(dynamic, 16)
+  for (size_t i = 0; i < n; ++i) {
+    const double *xi = pos + 3 * i;
+    const double si = rad[i];
+    const double zs = 1.875 * M_1_PI / pow(1.0, 7.5) / pow(si, 3);
+    double k[3] = {zs * vor[3 * i], zs * vor[3 * i + 1], zs * vor[3 * i + 2]};
+    for (size_t j = 0; j < n; ++j) {
+      if (j == i) continue;
+      const double *xj = pos + 3 * j;
+      const double d[3] = {xi[0] - xj[0], xi[1] - xj[1], xi[2] - xj[2]};
+      const double rho = sqrt(dot3(d, d));
+      const double sj = rad[j];
+      const double sigma = sqrt(0.5 * (si * si + sj * sj));
+      const double rho_bar = rho / sigma;
+      const double z = 1.875 * M_1_PI / pow(rho_bar * rho_bar + 1.0, 7.5) / pow(sigma, 3);
+      for (int c = 0; c < 3; ++c) k[c] += z * vor[3 * j + c];
+    }
+    for (int c = 0; c < 3; ++c) field[3 * i + c] = k[c];
+  }
+}

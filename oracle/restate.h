@@ -33,6 +33,11 @@ void orc_linear_diagnostics(size_t n, const double *pos, const double *vor, doub
 
 double orc_enstrophy(size_t n, const double *pos, const double *vor, const double *rad);
 double orc_helicity(size_t n, const double *pos, const double *vor, const double *rad);
+/* Smoothed vorticity field of every particle (N x 3):
+ *   K_i = Z(0, s_i) alpha_i + sum_{j != i} Z(rho_ij, sigma_ij) alpha_j. */
+void orc_influence(size_t n, const double *pos, const double *vor, const double *rad,
+                   double *field);
+
 /* wake_id[i] is the wake a particle belongs to (pairs inside one wake are
  * weighted twice as much as pairs across wakes, as the reference does). */
 double orc_kinetic_energy(size_t n, const int32_t *wake_id, const double *pos,

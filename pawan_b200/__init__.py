@@ -110,6 +110,7 @@ _SIGS = {
     "pawan_system_euler": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_size_t]),
     "pawan_system_diagnose": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
     "pawan_system_kinetic_energy": (ctypes.c_int, [_vp, _dp]),
+    "pawan_system_influence": (ctypes.c_int, [_vp, _dp, ctypes.c_size_t]),
     "pawan_system_set_nu": (ctypes.c_int, [_vp, ctypes.c_double]),
     "pawan_system_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pawan_system_write_frame": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_double, ctypes.c_int]),
@@ -362,6 +363,13 @@ class System:
         v = ctypes.c_double()
         self.ctx.check(self._lib.pawan_system_kinetic_energy(self._h, ctypes.byref(v)))
         return v.value
+
+    def influence(self) -> np.ndarray:
+        """Vorticity field of every particle (N x 3, FP64): the reference's
+        ``__interaction::resolve()`` / ``influence()``."""
+        k = np.empty((self.n, 3))
+        self.ctx.check(self._lib.pawan_system_influence(self._h, _p(k), k.size))
+        return k
 
     def set_nu(self, nu: float):
         self.ctx.check(self._lib.pawan_system_set_nu(self._h, float(nu)))

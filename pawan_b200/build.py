@@ -34,8 +34,8 @@ PER_FILE = {
     "noalloc.cu": ["--ftz=true"],
     "pair_plain.cu": ["--fmad=false"],
 }
-SOURCES = ["pair_f32.cu", "pair_f64.cu", "pair_plain.cu", "stage.cu", "diag.cu", "peak.cu",
-           "runtime.cpp", "serve.cpp", "noalloc.cu"]
+SOURCES = ["pair_f32.cu", "pair_f64.cu", "pair_plain.cu", "stage.cu", "diag.cu", "influence.cu",
+           "peak.cu", "runtime.cpp", "serve.cpp", "noalloc.cu"]
 
 
 def nvcc() -> str:

@@ -56,6 +56,10 @@ cudaError_t launch_diagnostics(int n, const double4 *pos64, const double4 *vor64
                                const int *wake_id, double *scratch, double *out, bool quadratic,
                                cudaStream_t s);
 
+// Vorticity field (FP64) of one system: field[3i..3i+2] = sum_j Z_ij alpha_j.
+cudaError_t launch_influence(int n, const double4 *pos64, const double4 *vor64, double *field,
+                             cudaStream_t s);
+
 // Throughput probes: FP32 FFMA and FP64 DFMA chains.  flops = launched FMAs * 2.
 cudaError_t launch_ffma_peak(int blocks, int threads, int iters, float *sink, cudaStream_t s);
 cudaError_t launch_dfma_peak(int blocks, int threads, int iters, double *sink, cudaStream_t s);

@@ -440,7 +440,7 @@ int system_alloc(pawan_system *sys) {
   const size_t n = sys->n;
   if (sys->ordered_alloc) {
     for (auto *b : {&sys->X, &sys->Xs, &sys->K1, &sys->K2, &sys->R, &sys->rad, &sys->vol,
-                    &sys->diag_scratch, &sys->diag_out, &sys->Xc})
+                    &sys->diag_scratch, &sys->diag_out, &sys->Xc, &sys->field})
       b->ordered_on(ctx->stream);
     sys->wake_id.ordered_on(ctx->stream);
     for (auto *b : {&sys->pos32, &sys->vor32, &sys->poslo, &sys->vorlo}) b->ordered_on(ctx->stream);
@@ -523,7 +523,7 @@ size_t pawan_system::device_bytes() const {
   return X.bytes() + Xs.bytes() + K1.bytes() + K2.bytes() + R.bytes() + rad.bytes() +
          vol.bytes() + wake_id.bytes() + pos32.bytes() + vor32.bytes() + poslo.bytes() +
          vorlo.bytes() + pos64.bytes() +
-         vor64.bytes() + diag_scratch.bytes() + diag_out.bytes() + Xc.bytes() +
+         vor64.bytes() + diag_scratch.bytes() + diag_out.bytes() + Xc.bytes() + field.bytes() +
          (plan ? plan->partial.bytes() : 0);
 }
 
@@ -898,6 +898,21 @@ int pawan_system_kinetic_energy(pawan_system *sys, double *ke) {
   double h[12];
   PAWAN_TRY(run_diagnostics(sys, true, h));
   *ke = h[11];
+  return PAWAN_OK;
+}
+
+int pawan_system_influence(pawan_system *sys, double *field, size_t size) {
+  CHECK_SYS(sys);
+  pawan_ctx *ctx = sys->ctx;
+  if (!field || size != 3 * sys->n) return fail(ctx, PAWAN_ERR_INVALID, "field size must be 3*N");
+  if (!sys->has_particles) return fail(ctx, PAWAN_ERR_STATE, "particles not set");
+  if (!sys->field.p) PAWAN_CUDA(ctx, sys->field.alloc(3 * sys->n));
+  // pos64 / vor64 hold pack(X) between API calls
+  PAWAN_CUDA(ctx, launch_influence((int)sys->n, sys->pos64.p, sys->vor64.p, sys->field.p, ctx->stream));
+  ctx->launches++;
+  PAWAN_CUDA(ctx, cudaMemcpyAsync(field, sys->field.p, 3 * sys->n * sizeof(double),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return PAWAN_OK;
 }
 

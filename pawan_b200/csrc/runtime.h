@@ -113,6 +113,7 @@ struct pawan_system {
   bool fixed_tile = false;
   pawan::TileChoice tile;
   pawan::DBuf<double> X, Xs, K1, K2, R, rad, vol, diag_scratch, diag_out, Xc;
+  pawan::DBuf<double> field;  // vorticity field (N x 3), allocated on first use
   pawan::DBuf<int> wake_id;
   pawan::DBuf<float4> pos32, vor32, poslo, vorlo;
   pawan::DBuf<double4> pos64, vor64;

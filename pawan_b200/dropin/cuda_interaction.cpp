@@ -124,6 +124,19 @@ void __cuda::interact() {
   }
 }
 
+void __cuda::influence() {
+  upload();
+  size_t n = 0;
+  for (auto *w : _wakes) n += w->_numParticles;
+  std::vector<double> k(3 * n);
+  check(pawan_system_influence(_sys, k.data(), k.size()), "influence");
+  size_t o = 0;
+  for (auto *w : _wakes) {
+    scatter_rows(k.data() + 3 * o, w->_vorticityfield);
+    o += w->_numParticles;
+  }
+}
+
 void __cuda::diagnose() {
   upload();
   double out[11];

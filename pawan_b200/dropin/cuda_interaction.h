@@ -56,6 +56,11 @@ class __cuda : public __interaction {
  protected:
   /* The whole-solve hook (interaction.h:106): every wake pair in one launch. */
   void interact() override;
+  /* The vorticity-field hook (interaction.h:112) behind resolve(): FP64 on the
+   * device, into every wake's _vorticityfield, so the reference's
+   * __resolve::rebuild (src/resolve/resolve.cpp:10-57) builds its influence
+   * matrix on the GPU. */
+  void influence() override;
 
  private:
   std::vector<__wake *> _wakes;

@@ -10,6 +10,8 @@
 #include "src/integration/rk4.h"
 #include "src/interaction/interaction.h"
 #include "src/io/io.h"
+#include "src/resolve/resolve.h"
+#include "src/wake/vring.h"
 
 namespace {
 
@@ -195,6 +197,68 @@ int dropin_integrate(int nw, const size_t *counts, const double *pos, const doub
     rk.integrate(G, &io);
     delete G;
     for (auto *w : W) delete w;
+    return 0;
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return 1;
+  }
+}
+
+// Vorticity field (N x 3, wake order) after resolve(): __cuda (gpu) and the
+// reference __interaction (cpu).
+int dropin_influence(int nw, const size_t *counts, const double *pos, const double *vor,
+                     const double *rad, const double *vol, double *gpu, double *cpu) {
+  try {
+    auto Wg = make_wakes(nw, counts, pos, vor, rad, vol);
+    auto Wc = make_wakes(nw, counts, pos, vor, rad, vol);
+    ReadCuda *G = make_cuda(Wg, 0.0, PAWAN_PREC_F32);
+    NuInteraction *R = new NuInteraction(0.0);
+    for (auto *w : Wc) R->addWake(w);
+    G->resolve();
+    R->resolve();
+    size_t o = 0;
+    for (size_t k = 0; k < Wg.size(); ++k) {
+      for (size_t i = 0; i < Wg[k]->_numParticles; ++i)
+        for (size_t d = 0; d < 3; ++d) {
+          gpu[3 * (o + i) + d] = gsl_matrix_get(Wg[k]->_vorticityfield, i, d);
+          cpu[3 * (o + i) + d] = gsl_matrix_get(Wc[k]->_vorticityfield, i, d);
+        }
+      o += Wg[k]->_numParticles;
+    }
+    delete G;
+    delete R;
+    for (auto *w : Wg) delete w;
+    for (auto *w : Wc) delete w;
+    return 0;
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return 1;
+  }
+}
+
+// The reference's __resolve::rebuild on a __vring(radius, core, layers):
+// driven through __cuda (gpu) and through the reference __interaction (cpu).
+// Writes data/temp.wakeinfluence under the cwd (twice).  The resolved
+// strength vectors (length (2 layers + 1)^2) land in gpu / cpu.
+int dropin_vring_resolve(double radius, double core, int layers, double *gpu, double *cpu) {
+  try {
+    pawan::__vring *Vg = new pawan::__vring(radius, core, layers);
+    pawan::__vring *Vc = new pawan::__vring(radius, core, layers);
+    ReadCuda *G = new ReadCuda(Vg, 0.0, PAWAN_PREC_F32, 0);
+    NuInteraction *R = new NuInteraction(0.0);
+    R->addWake(Vc);
+    pawan::__io io;
+    pawan::__resolve rs;
+    rs.rebuild(G, &io);
+    rs.rebuild(R, &io);
+    gsl_vector_view vg = gsl_vector_view_array(gpu, G->_size);
+    gsl_vector_view vc = gsl_vector_view_array(cpu, R->_size);
+    G->getStates(&vg.vector);
+    R->getStates(&vc.vector);
+    delete G;
+    delete R;
+    delete Vg;
+    delete Vc;
     return 0;
   } catch (const std::exception &e) {
     std::fprintf(stderr, "%s\n", e.what());

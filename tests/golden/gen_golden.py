@@ -5,7 +5,7 @@ into oracle/_ref/libpawan_ref.so by `make -C oracle`) on small seeded inputs
 and stores inputs and outputs.  The fixtures pin the oracle restatement and the
 GPU path on machines without the reference tree (the GPU box).
 
-    python tests/golden/gen_golden.py
+    python tests/golden/gen_golden.py [case ...]     (no case: all of them)
 
 Cases (all FP64, reference layout for states/rates):
   ring64_solve       one ring, 8 stations x 8, nu = 0       __interaction::solve
@@ -16,6 +16,10 @@ Cases (all FP64, reference layout for states/rates):
   pair64_euler       2 x __integration::step, dt = 0.005
   pair64_diag        __interaction::diagnose + kinetic energy
   ring16_integrate   __rk4(0.02, 2).integrate -> data/temp.wake bytes
+  pair64_influence   __interaction::resolve -> influence: the vorticity field
+  vring1_influence   the same on the reference's __vring(1.0, 0.1, 1) (855
+                     particles) with seeded layer strengths
+  vring1_resolve     __resolve::rebuild on __vring(1.0, 0.1, 1): resolved strengths
 """
 from __future__ import annotations
 
@@ -44,10 +48,16 @@ def _save(name, **arrays):
     print("wrote", name)
 
 
-def main():
+def main(only=()):
     if not oracle.ref_available():
         raise SystemExit("oracle/_ref/libpawan_ref.so is not built (make -C oracle)")
     oracle.ref_set_threads(1)
+    global _save
+    write = _save
+
+    def _save(name, **arrays):  # noqa: F811 - restricted to the requested cases
+        if not only or name in only:
+            write(name, **arrays)
 
     ring = g.single_ring(n_stations=8, seed=11)
     pair = g.ring_pair(n_stations=4, seed=12, nu=1e-3)
@@ -89,6 +99,31 @@ def main():
     _save("ring16_integrate", wake_bytes=np.frombuffer(raw, dtype=np.uint8), T=np.float64(0.02),
           nsteps=np.int64(2), **d)
 
+    d = _inputs(pair)
+    ref = oracle.RefSystem(pair.counts, d["pos"], d["vor"], d["rad"], d["vol"], pair.nu)
+    _save("pair64_influence", field=ref.influence(), **d)
+
+    v = oracle.RefVring(1.0, 0.1, 1)
+    strengths = np.random.default_rng(15).uniform(0.5, 1.5, v.size)
+    v.set_states(strengths)
+    pos, vor, rad, vol = v.particles()
+    _save("vring1_influence", strengths=strengths, pos=pos, vor=vor, rad=rad, vol=vol,
+          counts=np.asarray([v.n], dtype=np.int64), field=v.influence())
+    v.close()
+
+    v = oracle.RefVring(1.0, 0.1, 1)
+    pos, vor, rad, vol = v.particles()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.makedirs(os.path.join(tmp, "data"))
+        os.chdir(tmp)
+        try:
+            resolved = v.resolve()
+        finally:
+            os.chdir(cwd)
+    _save("vring1_resolve", radius=np.float64(1.0), core=np.float64(0.1), layers=np.int64(1),
+          pos=pos, rad=rad, vol=vol, strengths=resolved)
+    v.close()
+
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

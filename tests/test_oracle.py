@@ -118,3 +118,43 @@ def test_conservation_of_total_vorticity_rate():
     d = load("pair64_solve")
     _, da = split_rates(d["counts"], d["rates"])
     assert np.abs(da.sum(axis=0)).max() < 1e-12 * np.abs(da).sum()
+
+
+@pytest.mark.parametrize("name", ["pair64_influence", "vring1_influence"])
+def test_restatement_matches_golden_influence(name):
+    """The vorticity field of __interaction::influence (interaction.cpp:110-155)."""
+    d = load(name)
+    k = oracle.influence(d["pos"], d["vor"], d["rad"])
+    assert rms_rel(k, d["field"]) < 1e-13 and max_rel(k, d["field"]) < 1e-12
+
+
+@needs_ref
+def test_restatement_influence_matches_reference_fresh_inputs():
+    sc = g.helical_wake(n_stations=3, seed=17, filaments=3, turns=1.0)
+    pos, vor, rad, vol = sc.union()
+    rad = rad * np.random.default_rng(3).uniform(0.8, 1.2, rad.shape)  # mixed radii
+    ref = oracle.RefSystem(sc.counts, pos, vor, rad, vol, 0.0)
+    k_ref = ref.influence()
+    k = oracle.influence(pos, vor, rad)
+    assert rms_rel(k, k_ref) < 1e-13 and max_rel(k, k_ref) < 1e-12
+
+
+@needs_ref
+def test_reference_vring_resolve_reproduces_golden():
+    """__resolve::rebuild on the reference's __vring (influence matrix by unit
+    strengths, LU solve against the ideal Gaussian core field) through the GSL
+    shim's LU routines."""
+    d = load("vring1_resolve")
+    v = oracle.RefVring(float(d["radius"]), float(d["core"]), int(d["layers"]))
+    pos, _, rad, vol = v.particles()
+    assert np.array_equal(pos, d["pos"]) and np.array_equal(rad, d["rad"])
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.makedirs(os.path.join(tmp, "data"))
+        os.chdir(tmp)
+        try:
+            s = v.resolve()
+        finally:
+            os.chdir(cwd)
+    v.close()
+    assert np.array_equal(s, d["strengths"])
