@@ -8,7 +8,7 @@ pair math with FP64 accumulation, FP64 RK4 state.  One step = one RK4 step =
 reference's symmetric loop evaluates N(N-1)/2 kernels per RHS for the same
 credit).  Seeded synthetic geometry (no dataset exists for this path).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pawan|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pawan|reference] [--strong]
 
 Prints one JSON line (rank 0).  `value` is device-timed throughput with the
 state resident in HBM; `e2e` is the same metric through the C ABI with host
@@ -18,7 +18,10 @@ FP32 FFMA throughput measured in the same run; `cpu_baseline` is the
 reference's own OpenMP __parallel::solve (compiled from its sources) on a
 bounded sample, on this host's cores.  With --gpus N (torchrun), every rank
 runs its own ring pair (independent replicas, weak scaling); the time is the
-max over ranks.
+max over ranks.  With --strong the ranks instead share ONE ring pair: each
+computes the rates of its block of targets and the blocks are all-gathered
+over NCCL on every RK4 stage (pawan_b200/shard.py); value is that one
+system's interactions over the slowest rank's time.
 """
 from __future__ import annotations
 
@@ -55,6 +58,9 @@ def parse():
     ap.add_argument("--no-suite", action="store_true", help="skip the batch and serving legs")
     ap.add_argument("--configs", action="store_true",
                     help="run every workload at its full length instead (minutes; one JSON line each)")
+    ap.add_argument("--strong", action="store_true",
+                    help="one system sharded over the ranks (all-gather per RK4 stage) instead of "
+                         "one replica per rank")
     ap.add_argument("--tile", default=None,
                     help="fixed FP32 tiling instead of the autotuned one: threads,threads_per_target,"
                          "targets_per_thread,unroll,blocks_per_sm,packed[,items_per_slot]")
@@ -511,6 +517,75 @@ def run_pawan(args, rk: Ranks):
         print(json.dumps(line), flush=True)
 
 
+def run_strong(args, rk: Ranks):
+    """One ring pair sharded over the ranks: strong scaling."""
+    import torch
+    from pawan_b200 import Context, System
+    from pawan_b200 import geometry as g
+    from pawan_b200.shard import ShardedSystem, torch_allgather
+    sc = g.ring_pair(n_stations=args.n_stations, steps=1)
+    N, dt = sc.n, sc.dt
+    ctx = Context(rk.local)
+    s = System.from_scenario(ctx, sc, "f32")
+    tuned = apply_tile(s, args.tile) if args.tile else s.get_config()
+    s.checkpoint()
+    sh = ShardedSystem(s, rk.rank, rk.world, torch_allgather() if rk.world > 1 else None)
+    for _ in range(args.warmup):
+        s.restore()
+        sh.rk4(dt, 1)
+        ctx.flush_l2()
+    ctx.synchronize()
+    rk.barrier()
+    ctx.synchronize()
+    clocks = ClockSampler(gpu_index(rk.local))
+    clocks.start()
+    ctx.profile(True)
+    launches0 = ctx.launch_count
+    ctx.mark(0)
+    for _ in range(args.steps):
+        s.restore()
+        sh.rk4(dt, 1)
+        ctx.flush_l2()
+    ctx.mark(1)
+    ms = ctx.elapsed_ms(0, 1)
+    ctx.synchronize()
+    launches = ctx.launch_count - launches0
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    clk = clocks.stop()
+    rk.barrier()
+    ms_max = rk.max(ms)
+    value = 4.0 * N * N * args.steps / (ms_max * 1e-3) / 1e9
+    st = s.get_states()
+    assert np.all(np.isfinite(st)), "non-finite state"
+    pair_avg_s = prof["pair_ms"] / max(1, prof["pair_launches"]) * 1e-3
+    flops = FLOPS_NU if sc.nu != 0 else FLOPS_NO_NU
+    own = prof["pair_interactions"] / max(1, prof["pair_launches"])
+    achieved = own * flops / pair_avg_s / 1e12
+    peak = ctx.peak_fp32(2.0) / 1e3
+    line = {"metric": METRIC, "value": value, "unit": "G interactions/s", "n_gpus": rk.world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded ring pair geometry, jitter 1e-4)",
+            "config": {"workload": f"leapfrogging coaxial ring pair, N={N}, nu={sc.nu}, dt={dt}, RK4 step",
+                       "n_particles": N, "precision": "fp32 pairs, fp64 accumulation+state",
+                       "parallelism": f"target shards x{rk.world} (NCCL all-gather of 48 B/particle per RK4 stage)",
+                       "shard_particles": sh.size, "allgather_bytes_per_step": 4 * 8 * 6 * sh.size * rk.world,
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "state": "restored to the initial geometry before every step (device copy)",
+                       "tile": tuned},
+            "gpu_launches": int(launches), "clocks": clk,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "pairs_f32_kernel",
+                         "flops_per_interaction": flops, "pair_launch_ms": pair_avg_s * 1e3,
+                         "peak_source": "measured: FFMA-chain probe (pawan_peak_fp32) in this run"}}
+    sh.close()
+    s.close()
+    ctx.close()
+    if rk.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def _finite_diag(d):
     return {k: (v.tolist() if hasattr(v, "tolist") else v) for k, v in d.items()}
 
@@ -606,6 +681,8 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rk)
+        elif args.strong:
+            run_strong(args, rk)
         else:
             run_pawan(args, rk)
     finally:

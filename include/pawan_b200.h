@@ -161,6 +161,33 @@ int pawan_system_restore(pawan_system *sys);
  * x = first 3N) for callers that keep data on the device. */
 int pawan_system_device_state(pawan_system *sys, double **state);
 
+/* ------------------------------------------------------- target sharding */
+/* One system over `world` processes, one GPU each.  No reference counterpart
+ * (the reference runs in one process); the reference's OpenMP path splits the
+ * targets of each source over threads (parallel.cpp:21), this splits them
+ * over GPUs.  Every process holds the whole state.  Process `rank` computes the
+ * rates of its block of targets [rank*S, min(N, (rank+1)*S)), S =
+ * pawan_shard_size(N, world) (a multiple of 512); the blocks are exchanged
+ * through caller-owned device buffers -- `send` (6*S doubles: this process's
+ * block) and `recv` (6*S*world doubles: every block in rank order, each laid
+ * out [6][S]) -- by an all-gather of send into recv on every process (e.g.
+ * torch.distributed / NCCL), ordered on the library's stream between the two
+ * calls below.  Every process then applies the same update to all N
+ * particles, so the states stay identical across processes.  One RK4 step:
+ * for stage in 1..4 { shard_rates; all-gather; shard_stage(stage) }.
+ * world = 0 clears the sharding; a sharded system refuses the unsharded
+ * solve / rk4 / euler and batches. */
+size_t pawan_shard_size(size_t n, int world);
+int pawan_system_set_shard(pawan_system *sys, int rank, int world, double *send, double *recv);
+/* Pair kernel over this process's targets, its block of rates into send. */
+int pawan_system_shard_rates(pawan_system *sys);
+/* After the all-gather: stage 1..4 of an RK4 step (rk4.cpp:24-66) for every
+ * particle from the gathered rates; stage 0 stores the rates (as a solve()). */
+int pawan_system_shard_stage(pawan_system *sys, int stage, double dt);
+/* The context's CUDA stream (cudaStream_t), for ordering a caller's
+ * collective with the library's kernels. */
+int pawan_ctx_stream(pawan_ctx *ctx, void **stream);
+
 /* ------------------------------------------------------------------ batch */
 /* Many independent systems in one persistent pair launch per RK4 stage
  * (ragged segments), the four stages optionally captured in a CUDA graph.

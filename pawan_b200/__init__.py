@@ -111,6 +111,11 @@ _SIGS = {
     "pawan_system_diagnose": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
     "pawan_system_kinetic_energy": (ctypes.c_int, [_vp, _dp]),
     "pawan_system_influence": (ctypes.c_int, [_vp, _dp, ctypes.c_size_t]),
+    "pawan_shard_size": (ctypes.c_size_t, [ctypes.c_size_t, ctypes.c_int]),
+    "pawan_system_set_shard": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
+    "pawan_system_shard_rates": (ctypes.c_int, [_vp]),
+    "pawan_system_shard_stage": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double]),
+    "pawan_ctx_stream": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
     "pawan_system_set_nu": (ctypes.c_int, [_vp, ctypes.c_double]),
     "pawan_system_set_precision": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pawan_system_write_frame": (ctypes.c_int, [_vp, ctypes.c_char_p, ctypes.c_double, ctypes.c_int]),
@@ -189,6 +194,13 @@ class Context:
 
     def _adopt(self, child):
         self._children.add(child)
+
+    @property
+    def stream(self) -> int:
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        s = _vp()
+        self.check(self._lib.pawan_ctx_stream(self._h, ctypes.byref(s)))
+        return int(s.value or 0)
 
     @property
     def handle(self):

@@ -80,6 +80,16 @@ struct StageDesc {
   int box_tile;      // 128 or 256 (divides kStageThreads)
   double ox, oy, oz; // origin the FP32 positions are relative to
   double dt;
+  // Target sharding over processes (null / 0 otherwise).  Process blocks of
+  // `shard` particles; this process's block starts at shard_first.  The
+  // exchange layout is [process][6][shard]: STAGE_SHARD writes this
+  // process's block to xchg_out, and when xchg_in is set (the all-gathered
+  // blocks of every process) the other modes read their rates from it
+  // instead of the partial chunks.
+  double *xchg_out;
+  const double *xchg_in;
+  int shard;
+  int shard_first;
 };
 
 enum StageMode : int {
@@ -90,6 +100,7 @@ enum StageMode : int {
   STAGE_FINAL = 4,   // x = x + ((k1 + r)*(dt/6) + (k2+k3)*(dt/3)); pack x
   STAGE_EULER = 5,   // x = x + r*dt; pack x   (integration.cpp:37-45)
   STAGE_PACK = 6,    // pack x only
+  STAGE_SHARD = 7,   // this process's block of rates -> xchg_out (no state change)
 };
 
 // 1/(4 pi) and friends.

@@ -109,6 +109,17 @@ static bool tile_supported(int precision, const PairConfig &pc) {
   return pairs_plain_supported(pc);
 }
 
+// Process blocks of a sharded system start at multiples of kShardAlign
+// particles: whole stage blocks and whole target tiles of every tiling.
+constexpr size_t kShardAlign = 512;
+
+static size_t shard_first(const pawan_system *y) { return (size_t)y->shard.rank * y->shard.size; }
+
+static size_t shard_count(const pawan_system *y) {
+  const size_t f = shard_first(y);
+  return f >= y->n ? 0 : std::min(y->shard.size, y->n - f);
+}
+
 // Work decomposition.  Target tiles of tb/p particles; sources in chunks of
 // whole tb-tiles sized so that the launch holds about `items_per_slot` items
 // per resident block (or of `fixed_chunk_sources` when > 0, which makes a
@@ -129,7 +140,8 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     p->geometry_versions.push_back(s->geometry_version);
     p->box_versions.push_back(~0ull);
     if (s->nu != 0.0) p->diffusion = true;
-    p->interactions += (double)s->n * (double)s->n;
+    const double targets = s->shard.active ? (double)shard_count(s) : (double)s->n;
+    p->interactions += targets * (double)s->n;
   }
   int bps = 0;
   PAWAN_TRY(occupancy(ctx, precision, tile.pc, p->diffusion, &bps));
@@ -161,11 +173,16 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     partial_total += (size_t)nch * 6 * (size_t)n;
     box_off[s] = box_total;
     box_total += 2 * (size_t)src_tiles;
+    // targets: all particles, or this process's block of a sharded system
+    // (block starts are multiples of kShardAlign, so of every TPB and TB)
+    const pawan_system *y = systems[s];
+    const int t_lo = y->shard.active ? (int)shard_first(y) : 0;
+    const int t_hi = y->shard.active ? t_lo + (int)shard_count(y) : n;
     for (int c = 0; c < nch; ++c) {
       const int s0 = c * tiles_per_chunk * TB;
       const int s1 = std::min(n, (c + 1) * tiles_per_chunk * TB);
-      for (int t0 = 0; t0 < n; t0 += TPB) {
-        const int nt = std::min(TPB, n - t0);
+      for (int t0 = t_lo; t0 < t_hi; t0 += TPB) {
+        const int nt = std::min(TPB, t_hi - t0);
         items.push_back({WorkItem{(int)s, t0, c, s0, s1}, (double)nt * (double)(s1 - s0)});
       }
     }
@@ -181,6 +198,7 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     p->items.ordered_on(ctx->stream);
     p->segs.ordered_on(ctx->stream);
     p->stage_items.ordered_on(ctx->stream);
+    p->shard_items.ordered_on(ctx->stream);
     p->stage_descs.ordered_on(ctx->stream);
   }
   PAWAN_CUDA(ctx, p->partial.alloc(partial_total));
@@ -188,7 +206,7 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
   std::vector<WorkItem> wh(items.size());
   for (size_t k = 0; k < items.size(); ++k) wh[k] = items[k].w;
   std::vector<SegDesc> sh(systems.size());
-  std::vector<StageItem> sih;
+  std::vector<StageItem> sih, shh;
   p->stage_host.resize(systems.size());
   for (size_t s = 0; s < systems.size(); ++s) {
     pawan_system *y = systems[s];
@@ -228,9 +246,18 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     g.oy = y->oy;
     g.oz = y->oz;
     g.dt = 0.0;
+    g.xchg_out = y->shard.active ? y->shard.send : nullptr;
+    g.xchg_in = y->shard.active ? y->shard.recv : nullptr;
+    g.shard = y->shard.active ? (int)y->shard.size : 0;
+    g.shard_first = y->shard.active ? (int)shard_first(y) : 0;
     for (int l0 = 0; l0 < d.n; l0 += kStageThreads) sih.push_back(StageItem{(int)s, l0});
+    if (y->shard.active) {
+      const int f = (int)shard_first(y), e = f + (int)shard_count(y);
+      for (int l0 = f; l0 < e; l0 += kStageThreads) shh.push_back(StageItem{(int)s, l0});
+    }
   }
   p->n_stage_blocks = (int)sih.size();
+  p->n_shard_blocks = (int)shh.size();
   p->dts.assign(systems.size(), 0.0);
   PAWAN_CUDA(ctx, p->items.alloc(wh.size()));
   PAWAN_CUDA(ctx, p->segs.alloc(sh.size()));
@@ -242,6 +269,11 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
                                   cudaMemcpyHostToDevice, ctx->stream));
   PAWAN_CUDA(ctx, cudaMemcpyAsync(p->stage_items.p, sih.data(), sih.size() * sizeof(StageItem),
                                   cudaMemcpyHostToDevice, ctx->stream));
+  if (!shh.empty()) {
+    PAWAN_CUDA(ctx, p->shard_items.alloc(shh.size()));
+    PAWAN_CUDA(ctx, cudaMemcpyAsync(p->shard_items.p, shh.data(), shh.size() * sizeof(StageItem),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+  }
   PAWAN_CUDA(ctx, cudaMemcpyAsync(p->stage_descs.p, p->stage_host.data(),
                                   p->stage_host.size() * sizeof(StageDesc), cudaMemcpyHostToDevice,
                                   ctx->stream));
@@ -821,8 +853,14 @@ int pawan_system_get_states(pawan_system *sys, double *state, size_t size) {
   return state_from_device(sys, sys->X.p, state);
 }
 
+#define CHECK_UNSHARDED(sys)                                                        \
+  if ((sys)->shard.active)                                                          \
+  return fail((sys)->ctx, PAWAN_ERR_STATE,                                          \
+              "system is sharded over processes: use pawan_system_shard_rates / shard_stage")
+
 int pawan_system_solve(pawan_system *sys) {
   CHECK_SYS(sys);
+  CHECK_UNSHARDED(sys);
   PAWAN_TRY(system_ensure_plan(sys));
   PAWAN_TRY(launch_pairs(sys->ctx, *sys->plan));
   return launch_stage_mode(sys->ctx, *sys->plan, STAGE_RATES);
@@ -852,6 +890,7 @@ int pawan_system_get_wake_rates(pawan_system *sys, size_t wake, double *velocity
 
 int pawan_system_rk4(pawan_system *sys, double dt, size_t nsteps) {
   CHECK_SYS(sys);
+  CHECK_UNSHARDED(sys);
   PAWAN_TRY(system_ensure_plan(sys));
   PAWAN_TRY(set_plan_dt(sys->ctx, *sys->plan, nullptr, dt));
   return rk4_steps(sys->ctx, *sys->plan, nsteps, false);
@@ -859,6 +898,7 @@ int pawan_system_rk4(pawan_system *sys, double dt, size_t nsteps) {
 
 int pawan_system_euler(pawan_system *sys, double dt, size_t nsteps) {
   CHECK_SYS(sys);
+  CHECK_UNSHARDED(sys);
   PAWAN_TRY(system_ensure_plan(sys));
   PAWAN_TRY(set_plan_dt(sys->ctx, *sys->plan, nullptr, dt));
   for (size_t k = 0; k < nsteps; ++k) {
@@ -913,6 +953,76 @@ int pawan_system_influence(pawan_system *sys, double *field, size_t size) {
   PAWAN_CUDA(ctx, cudaMemcpyAsync(field, sys->field.p, 3 * sys->n * sizeof(double),
                                   cudaMemcpyDeviceToHost, ctx->stream));
   PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PAWAN_OK;
+}
+
+size_t pawan_shard_size(size_t n, int world) {
+  if (world < 1 || n == 0) return 0;
+  const size_t per = (n + (size_t)world - 1) / (size_t)world;
+  return (per + kShardAlign - 1) / kShardAlign * kShardAlign;
+}
+
+static bool device_pointer(const void *p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int pawan_system_set_shard(pawan_system *sys, int rank, int world, double *send, double *recv) {
+  CHECK_SYS(sys);
+  pawan_ctx *ctx = sys->ctx;
+  if (world == 0) {
+    sys->shard = pawan_system::Shard{};
+    sys->plan.reset();
+    return PAWAN_OK;
+  }
+  if (world < 1 || rank < 0 || rank >= world)
+    return fail(ctx, PAWAN_ERR_INVALID, "shard rank must be in [0, world)");
+  if (!send || !recv || !device_pointer(send) || !device_pointer(recv))
+    return fail(ctx, PAWAN_ERR_INVALID, "shard exchange buffers must be device memory");
+  pawan_system::Shard sh;
+  sh.active = true;
+  sh.rank = rank;
+  sh.world = world;
+  sh.size = pawan_shard_size(sys->n, world);
+  sh.send = send;
+  sh.recv = recv;
+  sys->shard = sh;
+  sys->plan.reset();  // the next plan covers this process's targets
+  return PAWAN_OK;
+}
+
+int pawan_system_shard_rates(pawan_system *sys) {
+  CHECK_SYS(sys);
+  if (!sys->shard.active) return fail(sys->ctx, PAWAN_ERR_STATE, "system is not sharded");
+  PAWAN_TRY(system_ensure_plan(sys));
+  Plan &p = *sys->plan;
+  PAWAN_TRY(launch_pairs(sys->ctx, p));
+  cudaError_t e = launch_stage(STAGE_SHARD, p.n_shard_blocks, p.shard_items.p, p.stage_descs.p,
+                               sys->ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(sys->ctx, e, "shard reduce launch");
+  if (p.n_shard_blocks > 0) sys->ctx->launches++;
+  return PAWAN_OK;
+}
+
+int pawan_system_shard_stage(pawan_system *sys, int stage, double dt) {
+  CHECK_SYS(sys);
+  if (!sys->shard.active) return fail(sys->ctx, PAWAN_ERR_STATE, "system is not sharded");
+  static const int modes[5] = {STAGE_RATES, STAGE_K1, STAGE_K2, STAGE_K3, STAGE_FINAL};
+  if (stage < 0 || stage > 4) return fail(sys->ctx, PAWAN_ERR_INVALID, "stage must be 0..4");
+  PAWAN_TRY(system_ensure_plan(sys));
+  Plan &p = *sys->plan;
+  if (stage > 0) PAWAN_TRY(set_plan_dt(sys->ctx, p, nullptr, dt));
+  return launch_stage_mode(sys->ctx, p, modes[stage]);
+}
+
+int pawan_ctx_stream(pawan_ctx *ctx, void **stream) {
+  CHECK_CTX(ctx);
+  if (!stream) return PAWAN_ERR_INVALID;
+  *stream = ctx->stream;
   return PAWAN_OK;
 }
 
@@ -1065,6 +1175,8 @@ int pawan_batch_create(pawan_ctx *ctx, size_t n, pawan_system *const *systems, p
       return fail(ctx, PAWAN_ERR_INVALID, "batch systems must share the context");
     if (systems[i]->precision != b->precision)
       return fail(ctx, PAWAN_ERR_INVALID, "batch systems must share one precision");
+    if (systems[i]->shard.active)
+      return fail(ctx, PAWAN_ERR_INVALID, "a sharded system cannot join a batch");
     b->systems.push_back(systems[i]);
   }
   b->tile = default_tile(b->precision);

@@ -126,6 +126,15 @@ struct pawan_system {
   // device buffers from the memory pool in the order of ctx->stream (systems
   // owned by the serving engine); the context must outlive the system
   bool ordered_alloc = false;
+  // target sharding over processes (pawan_system_set_shard): this process
+  // computes the rates of particles [rank * size, min(n, (rank + 1) * size))
+  struct Shard {
+    bool active = false;
+    int rank = 0, world = 1;
+    size_t size = 0;         // particles per process block
+    double *send = nullptr;  // device, 6 * size: this process's block
+    double *recv = nullptr;  // device, 6 * size * world: every block, gathered
+  } shard;
   size_t device_bytes() const;
 };
 
@@ -151,6 +160,8 @@ struct Plan {
   DBuf<WorkItem> items;
   DBuf<SegDesc> segs;
   DBuf<StageItem> stage_items;
+  DBuf<StageItem> shard_items;  // the stage blocks of this process's targets
+  int n_shard_blocks = 0;
   DBuf<StageDesc> stage_descs;
   std::vector<StageDesc> stage_host;
   std::vector<double> dts;  // dt in the device stage table

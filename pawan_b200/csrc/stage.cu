@@ -10,6 +10,9 @@
 //   x3 = k3*dt + x              (:49-51)      STAGE_K3 (also forms k2 + k3, :61)
 //   x += (k1 + k4)*(dt/6) + (k2 + k3)*(dt/3)   (:58-66)   STAGE_FINAL
 // and __integration::step (src/integration/integration.cpp:37-45): x += r*dt.
+// For a system sharded over processes, STAGE_SHARD writes this process's
+// block of reduced rates to the exchange buffer, and after the all-gather the
+// stage modes read every particle's rates from the gathered buffer.
 // Products and sums use __dmul_rn/__dadd_rn so no multiply-add is contracted,
 // keeping the update bit-identical to the reference's for equal rates.
 #include "device.cuh"
@@ -90,13 +93,28 @@ __global__ void __launch_bounds__(kStageThreads)
 
   double r[6] = {0, 0, 0, 0, 0, 0};
   if (MODE != STAGE_PACK && has) {
+    if (MODE != STAGE_SHARD && d.xchg_in) {
+      const size_t S = (size_t)d.shard;
+      const double *g = d.xchg_in + ((size_t)l / S) * 6 * S + (size_t)l % S;
 #pragma unroll
-    for (int k = 0; k < 6; ++k) r[k] = d.partial[(size_t)k * n + l];
-    for (int c = 1; c < d.nchunks; ++c) {
-      const double *p = d.partial + (size_t)c * 6 * n + l;
+      for (int k = 0; k < 6; ++k) r[k] = g[(size_t)k * S];
+    } else {
 #pragma unroll
-      for (int k = 0; k < 6; ++k) r[k] = __dadd_rn(r[k], p[(size_t)k * n]);
+      for (int k = 0; k < 6; ++k) r[k] = d.partial[(size_t)k * n + l];
+      for (int c = 1; c < d.nchunks; ++c) {
+        const double *p = d.partial + (size_t)c * 6 * n + l;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) r[k] = __dadd_rn(r[k], p[(size_t)k * n]);
+      }
     }
+  }
+  if (MODE == STAGE_SHARD) {
+    if (has) {
+      double *o = d.xchg_out + (l - d.shard_first);
+#pragma unroll
+      for (int k = 0; k < 6; ++k) o[(size_t)k * d.shard] = r[k];
+    }
+    return;
   }
 
   // Per-segment step size; the coefficients are formed as the reference forms
@@ -182,6 +200,9 @@ cudaError_t launch_stage(int mode, int n_blocks, const StageItem *items, const S
       break;
     case STAGE_PACK:
       stage_kernel<STAGE_PACK><<<grid, block, 0, s>>>(items, descs);
+      break;
+    case STAGE_SHARD:
+      stage_kernel<STAGE_SHARD><<<grid, block, 0, s>>>(items, descs);
       break;
     default:
       return cudaErrorInvalidValue;
