@@ -131,6 +131,18 @@ int pawan_system_euler(pawan_system *sys, double dt, size_t nsteps);
  * [9] enstrophy, [10] helicity.  quadratic = 0 skips the O(N^2) terms
  * (out[9], out[10] then 0). */
 int pawan_system_diagnose(pawan_system *sys, double *out, int quadratic);
+/* Smoothing kernel: PAWAN_KERNEL_HIGHORDER (src/interaction/highorder.h, the
+ * reference's default) or PAWAN_KERNEL_GAUSSIAN (src/interaction/gaussian.h,
+ * which the reference selects with #define GAUSSIAN 1 in
+ * interaction_utils.h:13-24).  Applies to solve, RK4/Euler, diagnostics (with
+ * the Gaussian kernel the enstrophy is 0, as the reference's ENST stub
+ * returns, gaussian.h:67-86) and the vorticity field.  Systems of one batch
+ * share their kernel; the serving engine and pawan_interact_noalloc use the
+ * high-order kernel. */
+#define PAWAN_KERNEL_HIGHORDER 0
+#define PAWAN_KERNEL_GAUSSIAN 1
+int pawan_system_set_kernel(pawan_system *sys, int kernel);
+int pawan_system_get_kernel(pawan_system *sys, int *kernel);
 /* calculateKineticEnergy over all wakes (interaction.cpp:351-383). */
 int pawan_system_kinetic_energy(pawan_system *sys, double *ke);
 /* __interaction::resolve -> influence (interaction.cpp:45-47, 110-155): the

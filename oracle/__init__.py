@@ -23,6 +23,9 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 REF_LIB = os.path.join(_HERE, "_ref", "libpawan_ref.so")
+# the same reference sources compiled with their Gaussian smoothing kernel
+REF_GAUSS_LIB = os.path.join(_HERE, "_ref", "libpawan_ref_gauss.so")
+KERNELS = {"highorder": 0, "gaussian": 1}
 RESTATE_LIB = os.path.join(_HERE, "liboracle.so")
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -39,20 +42,20 @@ def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
-_ref = None
+_ref = {}
 _orc = None
 
 
-def ref_available() -> bool:
-    return os.path.exists(REF_LIB)
+def ref_available(kernel: str = "highorder") -> bool:
+    return os.path.exists(REF_GAUSS_LIB if kernel == "gaussian" else REF_LIB)
 
 
-def _load_ref():
-    global _ref
-    if _ref is None:
-        if not ref_available():
-            raise FileNotFoundError(f"{REF_LIB} not built (make -C oracle)")
-        lib = ctypes.CDLL(REF_LIB)
+def _load_ref(kernel: str = "highorder"):
+    if kernel not in _ref:
+        path = REF_GAUSS_LIB if kernel == "gaussian" else REF_LIB
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{path} not built (make -C oracle)")
+        lib = ctypes.CDLL(path)
         lib.refh_create.restype = ctypes.c_void_p
         lib.refh_create.argtypes = [ctypes.c_int, _szp, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int]
         lib.refh_destroy.argtypes = [ctypes.c_void_p]
@@ -81,8 +84,8 @@ def _load_ref():
         lib.refh_set_threads.argtypes = [ctypes.c_int]
         lib.refh_max_threads.restype = ctypes.c_int
         lib.refh_wtime.restype = ctypes.c_double
-        _ref = lib
-    return _ref
+        _ref[kernel] = lib
+    return _ref[kernel]
 
 
 def _load_orc():
@@ -99,6 +102,7 @@ def _load_orc():
             getattr(lib, name).restype = ctypes.c_double
             getattr(lib, name).argtypes = [ctypes.c_size_t, _dp, _dp, _dp]
         lib.orc_influence.argtypes = [ctypes.c_size_t, _dp, _dp, _dp, _dp]
+        lib.orc_set_kernel.argtypes = [ctypes.c_int]
         lib.orc_kinetic_energy.restype = ctypes.c_double
         lib.orc_kinetic_energy.argtypes = [ctypes.c_size_t, _i32p, _dp, _dp, _dp]
         _orc = lib
@@ -109,8 +113,9 @@ class RefSystem:
     """The reference's ``__interaction`` (serial) or ``__parallel`` (OpenMP)
     over wakes built from arrays, with viscosity ``nu``."""
 
-    def __init__(self, counts: Sequence[int], pos, vor, rad, vol, nu: float, parallel: bool = False):
-        lib = _load_ref()
+    def __init__(self, counts: Sequence[int], pos, vor, rad, vol, nu: float, parallel: bool = False,
+                 kernel: str = "highorder"):
+        lib = _load_ref(kernel)
         self._lib = lib
         self.counts = [int(c) for c in counts]
         self.n = sum(self.counts)
@@ -237,9 +242,15 @@ def ref_wtime() -> float:
 
 # ----------------------------------------------------------------- restatement
 
-def pairs(pos, vor, rad, vol, nu: float, targets=None):
-    """(velocity, vorticity rate) of `targets` (all when None), FP64."""
+def _restate(kernel: str = "highorder"):
     lib = _load_orc()
+    lib.orc_set_kernel(KERNELS[kernel])
+    return lib
+
+
+def pairs(pos, vor, rad, vol, nu: float, targets=None, kernel: str = "highorder"):
+    """(velocity, vorticity rate) of `targets` (all when None), FP64."""
+    lib = _restate(kernel)
     pos, vor, rad, vol = _f64(pos), _f64(vor), _f64(rad), _f64(vol)
     n = rad.shape[0]
     if targets is None:
@@ -252,8 +263,8 @@ def pairs(pos, vor, rad, vol, nu: float, targets=None):
     return u, da
 
 
-def rk4_step(pos, vor, rad, vol, nu: float, dt: float, nsteps: int = 1):
-    lib = _load_orc()
+def rk4_step(pos, vor, rad, vol, nu: float, dt: float, nsteps: int = 1, kernel: str = "highorder"):
+    lib = _restate(kernel)
     p, v = _f64(pos).copy(), _f64(vor).copy()
     rad, vol = _f64(rad), _f64(vol)
     for _ in range(nsteps):
@@ -269,21 +280,21 @@ def linear_diagnostics(pos, vor):
     return out[0:3], out[3:6], out[6:9]
 
 
-def enstrophy(pos, vor, rad) -> float:
+def enstrophy(pos, vor, rad, kernel: str = "highorder") -> float:
     pos, vor, rad = _f64(pos), _f64(vor), _f64(rad)
-    return float(_load_orc().orc_enstrophy(rad.shape[0], _ptr(pos), _ptr(vor), _ptr(rad)))
+    return float(_restate(kernel).orc_enstrophy(rad.shape[0], _ptr(pos), _ptr(vor), _ptr(rad)))
 
 
-def helicity(pos, vor, rad) -> float:
+def helicity(pos, vor, rad, kernel: str = "highorder") -> float:
     pos, vor, rad = _f64(pos), _f64(vor), _f64(rad)
-    return float(_load_orc().orc_helicity(rad.shape[0], _ptr(pos), _ptr(vor), _ptr(rad)))
+    return float(_restate(kernel).orc_helicity(rad.shape[0], _ptr(pos), _ptr(vor), _ptr(rad)))
 
 
-def influence(pos, vor, rad) -> np.ndarray:
+def influence(pos, vor, rad, kernel: str = "highorder") -> np.ndarray:
     """Vorticity field K_i = Z(0, s_i) alpha_i + sum_j Z_ij alpha_j (N x 3), FP64."""
     pos, vor, rad = _f64(pos), _f64(vor), _f64(rad)
     k = np.empty((rad.shape[0], 3))
-    _load_orc().orc_influence(rad.shape[0], _ptr(pos), _ptr(vor), _ptr(rad), _ptr(k))
+    _restate(kernel).orc_influence(rad.shape[0], _ptr(pos), _ptr(vor), _ptr(rad), _ptr(k))
     return k
 
 

@@ -15,8 +15,42 @@
 #include <stdlib.h>
 #include <string.h>
 
+/* Smoothing kernel: 0 = high-order algebraic (highorder.h, the reference's
+ * default), 1 = Gaussian (gaussian.h).  Set by orc_set_kernel. */
+static int g_kernel = 0;
+
+void orc_set_kernel(int kernel) { g_kernel = kernel; }
+
+/* gaussian.h:20-23 (ZETASIG). */
+static double zeta_gauss(double rho, double sigma) {
+  const double rho_bar = rho / sigma;
+  return exp(-0.5 * rho_bar * rho_bar) / pow(sigma, 3.0) / pow(2.0 * M_PI, 1.5);
+}
+
+/* gaussian.h:46-59 (KERNEL): q, F and Z of one pair. */
+static void kernel_qfz_gauss(double rho, double sigma, double *q, double *F, double *Z) {
+  const double rho_bar = rho / sigma;
+  const double sig3 = sigma * sigma * sigma;
+  const double z = zeta_gauss(rho, sigma);
+  const double phi = 0.25 * M_1_PI * erf(M_SQRT1_2 * rho_bar) / sig3;
+  *Z = z;
+  *q = (phi / rho_bar - z) / (rho_bar * rho_bar);
+  *F = (z - 3.0 * (*q)) / (rho * rho);
+}
+
+/* highorder.h:20-23 (ZETASIG), or the Gaussian one. */
+static double zeta(double rho, double sigma) {
+  if (g_kernel == 1) return zeta_gauss(rho, sigma);
+  const double rho_bar = rho / sigma;
+  return 1.875 * M_1_PI / pow(rho_bar * rho_bar + 1.0, 7.5) / pow(sigma, 3);
+}
+
 /* highorder.h:48-60 (KERNEL) and :20-23 (ZETASIG): q, F and Z of one pair. */
 static void kernel_qfz(double rho, double sigma, double *q, double *F, double *Z) {
+  if (g_kernel == 1) {
+    kernel_qfz_gauss(rho, sigma, q, F, Z);
+    return;
+  }
   const double rho_bar = rho / sigma;
   const double z = 1.875 * M_1_PI / pow(rho_bar * rho_bar + 1.0, 7.5) / pow(sigma, 3);
   const double rho_bar2 = rho_bar * rho_bar;
@@ -152,6 +186,7 @@ void orc_linear_diagnostics(size_t n, const double *pos, const double *vor, doub
  * i<j, pairs across wakes twice over all (i,j); both equal one count per
  * ordered pair, which is how the sum is written here. */
 double orc_enstrophy(size_t n, const double *pos, const double *vor, const double *rad) {
+  if (g_kernel == 1) return 0.0; /* gaussian.h:67-86: ENST is a stub returning 0 */
   double total = 0.0;
 #pragma omp parallel for reduction(+ : total) schedule(dynamic, 16)
   for (long il = 0; il < (long)n; ++il) {
@@ -239,7 +274,7 @@ void orc_influence(size_t n, const double *pos, const double *vor, const double 
   for (size_t i = 0; i < n; ++i) {
     const double *xi = pos + 3 * i;
     const double si = rad[i];
-    const double zs = 1.875 * M_1_PI / pow(1.0, 7.5) / pow(si, 3);
+    const double zs = zeta(0.0, si);
     double k[3] = {zs * vor[3 * i], zs * vor[3 * i + 1], zs * vor[3 * i + 2]};
     for (size_t j = 0; j < n; ++j) {
       if (j == i) continue;
@@ -248,8 +283,7 @@ void orc_influence(size_t n, const double *pos, const double *vor, const double 
       const double rho = sqrt(dot3(d, d));
       const double sj = rad[j];
       const double sigma = sqrt(0.5 * (si * si + sj * sj));
-      const double rho_bar = rho / sigma;
-      const double z = 1.875 * M_1_PI / pow(rho_bar * rho_bar + 1.0, 7.5) / pow(sigma, 3);
+      const double z = zeta(rho, sigma);
       for (int c = 0; c < 3; ++c) k[c] += z * vor[3 * j + c];
     }
     for (int c = 0; c < 3; ++c) field[3 * i + c] = k[c];

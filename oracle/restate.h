@@ -17,6 +17,11 @@
 extern "C" {
 #endif
 
+/* Smoothing kernel of every function below: 0 = high-order algebraic
+ * (src/interaction/highorder.h, the reference's default), 1 = Gaussian
+ * (src/interaction/gaussian.h). */
+void orc_set_kernel(int kernel);
+
 /* Velocity and vorticity rate of the targets listed in `targets` (or all N when
  * targets == NULL, nt == N), summed over every source j != target. */
 void orc_pairs(size_t n, const double *pos, const double *vor, const double *rad,

@@ -31,6 +31,7 @@ HEADER = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))
                       "pawan_b200.h")
 
 PREC = {"f32": 0, "f64": 1, "f64_plain": 2}
+KERNELS = {"highorder": 0, "gaussian": 1}  # PAWAN_KERNEL_*
 OK = 0
 STATUS = {0: "ok", 1: "invalid argument", 2: "cuda error", 3: "out of memory", 4: "invalid state",
           5: "exceeds budget", 6: "timeout", 7: "not found", 8: "rejected"}
@@ -112,6 +113,8 @@ _SIGS = {
     "pawan_system_kinetic_energy": (ctypes.c_int, [_vp, _dp]),
     "pawan_system_influence": (ctypes.c_int, [_vp, _dp, ctypes.c_size_t]),
     "pawan_shard_size": (ctypes.c_size_t, [ctypes.c_size_t, ctypes.c_int]),
+    "pawan_system_set_kernel": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pawan_system_get_kernel": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     "pawan_system_set_shard": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "pawan_system_shard_rates": (ctypes.c_int, [_vp]),
     "pawan_system_shard_stage": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double]),
@@ -375,6 +378,16 @@ class System:
         v = ctypes.c_double()
         self.ctx.check(self._lib.pawan_system_kinetic_energy(self._h, ctypes.byref(v)))
         return v.value
+
+    def set_kernel(self, kernel: str):
+        """Smoothing kernel: "highorder" (the reference's default) or "gaussian"."""
+        self.ctx.check(self._lib.pawan_system_set_kernel(self._h, KERNELS[kernel]))
+
+    @property
+    def kernel(self) -> str:
+        k = ctypes.c_int()
+        self.ctx.check(self._lib.pawan_system_get_kernel(self._h, ctypes.byref(k)))
+        return {v: n for n, v in KERNELS.items()}[k.value]
 
     def influence(self) -> np.ndarray:
         """Vorticity field of every particle (N x 3, FP64): the reference's

@@ -103,9 +103,20 @@ enum StageMode : int {
   STAGE_SHARD = 7,   // this process's block of rates -> xchg_out (no state change)
 };
 
+// Smoothing kernel of a system: the reference's high-order algebraic kernel
+// (src/interaction/highorder.h, its default) or its Gaussian one
+// (src/interaction/gaussian.h, selected there by #define GAUSSIAN).
+enum SmoothingKernel : int {
+  KERNEL_HIGHORDER = 0,
+  KERNEL_GAUSSIAN = 1,
+};
+
 // 1/(4 pi) and friends.
 constexpr double kInv4Pi = 0.07957747154594766788;
 constexpr double kInvPi = 0.31830988618379067154;
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kSqrt2OverPi = 0.79788456080286535588;  // sqrt(2/pi)
+constexpr double kSqrtHalf = 0.70710678118654752440;     // 1/sqrt(2)
 
 // Block sizes.  Source tiles (and so bounding boxes) are 128 or 256
 // particles; stage blocks cover whole tiles.

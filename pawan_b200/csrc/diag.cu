@@ -12,6 +12,10 @@
 //   kinetic energy   2 sum_i |a_i|^2/(8 pi s_i) + sum_{i != j} w_ij KE_ij with
 //                    w_ij = 2 inside a wake, 1 across wakes      :351-383,
 //                    KINETICENERGY (interaction_utils.h:197-240)
+// With the Gaussian kernel (src/interaction/gaussian.h) the enstrophy terms
+// are the reference's stub ENST = 0 (gaussian.h:67-86) and helicity uses the
+// Gaussian QSIG (:30-38): q = (phi/rho_bar - Z)/rho_bar^2 with
+// phi = erf(rho_bar/sqrt 2)/(4 pi sigma^3), Z = exp(-rho_bar^2/2)/(sigma^3 (2 pi)^1.5).
 // The reference's pair loops visit i<j and double (or, across wakes, double
 // the full cross sum); both equal one term per ordered pair, which is the
 // gather sum written here.  Per-target sums are reduced per block in a fixed
@@ -71,6 +75,7 @@ __global__ void __launch_bounds__(kDiagThreads)
   block_sum<kLin>(v, smem, block_out + (size_t)blockIdx.x * kLin);
 }
 
+template <int KERN>
 __global__ void __launch_bounds__(kDiagThreads)
     diag_quadratic_kernel(int n, const double4 *__restrict__ pos, const double4 *__restrict__ vor,
                           const int *__restrict__ wake_id, double *__restrict__ block_out) {
@@ -92,7 +97,7 @@ __global__ void __launch_bounds__(kDiagThreads)
   const double si = ri.w;
   const double hi = 0.5 * si * si;
   const double a2 = ai.x * ai.x + ai.y * ai.y + ai.z * ai.z;
-  double ens = valid ? 5.0 * kInvPi / 4.0 / (si * si * si) * a2 : 0.0;
+  double ens = (valid && KERN == KERNEL_HIGHORDER) ? 5.0 * kInvPi / 4.0 / (si * si * si) * a2 : 0.0;
   double hel = 0.0;
   double ke = valid ? 2.0 * (kInvPi * a2 / si / 8.0) : 0.0;
 
@@ -117,18 +122,29 @@ __global__ void __launch_bounds__(kDiagThreads)
       const double aa = ai.x * aj.x + ai.y * aj.y + ai.z * aj.z;
       const double aix = ai.x * x0 + ai.y * x1 + ai.z * x2;
       const double ajx = aj.x * x0 + aj.y * x1 + aj.z * x2;
-      // ENST: factor = (1/8pi) (rho^2 + sigma^2)^(-7/2)
-      const double factor = (kInvPi / 8.0) * (w4 * w3);
-      const double F1 = factor * (10.0 * sig2 * sig2 - 2.0 * rho2 * rho2 - 7.0 * sig2 * rho2);
-      const double F2 = factor * (-15.0 * rho2);
-      ens += F1 * aa + F2 * aix * ajx;
-      // QSIG: q = (phi/rho_bar - Z)/rho_bar^2
       const double rinv = rsqrt(rho2);
-      const double uu = sig2 * w2;
-      const double u2 = uu * uu;
-      const double zc = u2 * u2 * u2 * w3;
-      const double ph = (rho2 + 1.5 * sig2) * w4 * rinv;
-      const double q = A * (ph - 7.5 * zc) * sig2 * (rinv * rinv);
+      double q;
+      if (KERN == KERNEL_GAUSSIAN) {
+        // QSIG, gaussian.h:30-38
+        const double sig = sqrt(sig2);
+        const double rho_bar = rho2 * rinv / sig;
+        const double sig3 = sig2 * sig;
+        const double z = exp(-0.5 * rho_bar * rho_bar) / sig3 / pow(2.0 * kPi, 1.5);
+        const double phi = 0.25 * kInvPi * erf(kSqrtHalf * rho_bar) / sig3;
+        q = (phi / rho_bar - z) / (rho_bar * rho_bar);
+      } else {
+        // ENST: factor = (1/8pi) (rho^2 + sigma^2)^(-7/2)
+        const double factor = (kInvPi / 8.0) * (w4 * w3);
+        const double F1 = factor * (10.0 * sig2 * sig2 - 2.0 * rho2 * rho2 - 7.0 * sig2 * rho2);
+        const double F2 = factor * (-15.0 * rho2);
+        ens += F1 * aa + F2 * aix * ajx;
+        // QSIG: q = (phi/rho_bar - Z)/rho_bar^2
+        const double uu = sig2 * w2;
+        const double u2 = uu * uu;
+        const double zc = u2 * u2 * u2 * w3;
+        const double ph = (rho2 + 1.5 * sig2) * w4 * rinv;
+        q = A * (ph - 7.5 * zc) * sig2 * (rinv * rinv);
+      }
       const double c0 = ai.y * aj.z - ai.z * aj.y;
       const double c1 = ai.z * aj.x - ai.x * aj.z;
       const double c2 = ai.x * aj.y - ai.y * aj.x;
@@ -178,7 +194,7 @@ size_t diag_scratch_doubles(int n) {
   return nblk * (kLin + kQuad);
 }
 
-cudaError_t launch_diagnostics(int n, const double4 *pos64, const double4 *vor64,
+cudaError_t launch_diagnostics(int n, int kernel, const double4 *pos64, const double4 *vor64,
                                const int *wake_id, double *scratch, double *out, bool quadratic,
                                cudaStream_t s) {
   if (n <= 0) return cudaErrorInvalidValue;
@@ -188,7 +204,10 @@ cudaError_t launch_diagnostics(int n, const double4 *pos64, const double4 *vor64
   diag_linear_kernel<<<nblk, kDiagThreads, 0, s>>>(n, pos64, vor64, lin);
   diag_final_kernel<kLin><<<1, kDiagThreads, 0, s>>>(nblk, lin, out, 0.0);
   if (quadratic) {
-    diag_quadratic_kernel<<<nblk, kDiagThreads, 0, s>>>(n, pos64, vor64, wake_id, quad);
+    if (kernel == KERNEL_GAUSSIAN)
+      diag_quadratic_kernel<KERNEL_GAUSSIAN><<<nblk, kDiagThreads, 0, s>>>(n, pos64, vor64, wake_id, quad);
+    else
+      diag_quadratic_kernel<KERNEL_HIGHORDER><<<nblk, kDiagThreads, 0, s>>>(n, pos64, vor64, wake_id, quad);
     diag_final_kernel<kQuad><<<1, kDiagThreads, 0, s>>>(nblk, quad, out, 0.0);
   }
   return cudaGetLastError();

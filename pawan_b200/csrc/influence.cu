@@ -12,7 +12,9 @@
 //   K_i = sum_j Z(rho_ij, sigma_ij) alpha_j   over every j, i included:
 // the j = i term has rho = 0 and sigma = s_i, which is SELFINFLUENCE.
 // With w = (rho^2 + sigma^2)^(-1/2) and u = sigma^2 w^2 = 1/(rho_bar^2 + 1):
-//   Z = (15 / 8 pi) sigma^-3 (rho_bar^2 + 1)^-7.5 = (15 / 8 pi) u^6 w^3.
+//   Z = (15 / 8 pi) sigma^-3 (rho_bar^2 + 1)^-7.5 = (15 / 8 pi) u^6 w^3,
+// or with the Gaussian kernel (src/interaction/gaussian.h:20-23)
+//   Z = exp(-rho_bar^2 / 2) / (sigma^3 (2 pi)^1.5).
 //
 // One thread per target (registers), sources staged through shared memory
 // in tiles, summed in source order: deterministic.  ~20 FP64 operations and
@@ -27,6 +29,7 @@ namespace {
 
 constexpr int kInfThreads = 128;
 
+template <int KERN>
 __global__ void __launch_bounds__(kInfThreads)
     influence_kernel(int n, const double4 *__restrict__ pos, const double4 *__restrict__ vor,
                      double *__restrict__ field) {
@@ -38,6 +41,7 @@ __global__ void __launch_bounds__(kInfThreads)
   const double4 ri = valid ? pos[i] : make_double4(0.0, 0.0, 0.0, 1.0);
   const double hi = 0.5 * ri.w * ri.w;
   const double c = 1.875 * kInvPi;  // 15 / (8 pi)
+  const double cg = 0.06349363593424096978;  // (2 pi)^-1.5
   double kx = 0.0, ky = 0.0, kz = 0.0;
   for (int ts = 0; ts < n; ts += kInfThreads) {
     __syncthreads();
@@ -53,12 +57,18 @@ __global__ void __launch_bounds__(kInfThreads)
       const double dx = ri.x - rj.x, dy = ri.y - rj.y, dz = ri.z - rj.z;
       const double rho2 = dx * dx + dy * dy + dz * dz;
       const double sig2 = hi + 0.5 * rj.w * rj.w;
-      const double w = rsqrt(rho2 + sig2);
-      const double w2 = w * w;
-      const double u = sig2 * w2;
-      const double u2 = u * u;
-      const double u6 = u2 * u2 * u2;
-      const double z = c * u6 * w2 * w;
+      double z;
+      if (KERN == KERNEL_GAUSSIAN) {
+        const double is = rsqrt(sig2);
+        z = exp(-0.5 * rho2 * is * is) * (is * is * is) * cg;
+      } else {
+        const double w = rsqrt(rho2 + sig2);
+        const double w2 = w * w;
+        const double u = sig2 * w2;
+        const double u2 = u * u;
+        const double u6 = u2 * u2 * u2;
+        z = c * u6 * w2 * w;
+      }
       kx += z * aj.x;
       ky += z * aj.y;
       kz += z * aj.z;
@@ -73,11 +83,14 @@ __global__ void __launch_bounds__(kInfThreads)
 
 }  // namespace
 
-cudaError_t launch_influence(int n, const double4 *pos64, const double4 *vor64, double *field,
-                             cudaStream_t s) {
+cudaError_t launch_influence(int n, int kernel, const double4 *pos64, const double4 *vor64,
+                             double *field, cudaStream_t s) {
   if (n <= 0) return cudaSuccess;
   const int blocks = (n + kInfThreads - 1) / kInfThreads;
-  influence_kernel<<<blocks, kInfThreads, 0, s>>>(n, pos64, vor64, field);
+  if (kernel == KERNEL_GAUSSIAN)
+    influence_kernel<KERNEL_GAUSSIAN><<<blocks, kInfThreads, 0, s>>>(n, pos64, vor64, field);
+  else
+    influence_kernel<KERNEL_HIGHORDER><<<blocks, kInfThreads, 0, s>>>(n, pos64, vor64, field);
   return cudaGetLastError();
 }
 

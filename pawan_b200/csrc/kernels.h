@@ -25,24 +25,28 @@ struct PairConfig {
 
 inline int targets_per_block(const PairConfig &c) { return c.tb / c.p * c.r; }
 
+// `kernel` below is a SmoothingKernel (device.cuh).
+
 // FP32 pair math, FP64 accumulation of per-tile partial sums.
-bool pairs_f32_supported(const PairConfig &c);
-cudaError_t pairs_f32_occupancy(const PairConfig &c, bool diffusion, int *blocks_per_sm);
-cudaError_t launch_pairs_f32(const PairConfig &c, bool diffusion, int grid, const WorkItem *items,
-                             int n_items, const SegDesc *segs, int *next_item, cudaStream_t s);
+bool pairs_f32_supported(const PairConfig &c, int kernel);
+cudaError_t pairs_f32_occupancy(const PairConfig &c, bool diffusion, int kernel, int *blocks_per_sm);
+cudaError_t launch_pairs_f32(const PairConfig &c, bool diffusion, int kernel, int grid,
+                             const WorkItem *items, int n_items, const SegDesc *segs,
+                             int *next_item, cudaStream_t s);
 
 // FP64 with the same algebra as the FP32 kernel ("tuned FP64").
-bool pairs_f64_supported(const PairConfig &c);
-cudaError_t pairs_f64_occupancy(const PairConfig &c, bool diffusion, int *blocks_per_sm);
-cudaError_t launch_pairs_f64(const PairConfig &c, bool diffusion, int grid, const WorkItem *items,
-                             int n_items, const SegDesc *segs, int *next_item, cudaStream_t s);
+bool pairs_f64_supported(const PairConfig &c, int kernel);
+cudaError_t pairs_f64_occupancy(const PairConfig &c, bool diffusion, int kernel, int *blocks_per_sm);
+cudaError_t launch_pairs_f64(const PairConfig &c, bool diffusion, int kernel, int grid,
+                             const WorkItem *items, int n_items, const SegDesc *segs,
+                             int *next_item, cudaStream_t s);
 
 // FP64, the reference's formula term by term (pow, divisions): the plain
 // FP64 comparator.
-bool pairs_plain_supported(const PairConfig &c);
-cudaError_t pairs_plain_occupancy(const PairConfig &c, int *blocks_per_sm);
-cudaError_t launch_pairs_plain(const PairConfig &c, int grid, const WorkItem *items, int n_items,
-                               const SegDesc *segs, int *next_item, cudaStream_t s);
+bool pairs_plain_supported(const PairConfig &c, int kernel);
+cudaError_t pairs_plain_occupancy(const PairConfig &c, int kernel, int *blocks_per_sm);
+cudaError_t launch_pairs_plain(const PairConfig &c, int kernel, int grid, const WorkItem *items,
+                               int n_items, const SegDesc *segs, int *next_item, cudaStream_t s);
 
 // Per-particle stage kernel (reduce partials, RK4 stage update, pack).
 cudaError_t launch_stage(int mode, int n_blocks, const StageItem *items, const StageDesc *descs,
@@ -52,13 +56,13 @@ cudaError_t launch_stage(int mode, int n_blocks, const StageItem *items, const S
 // doubles; out[0..10] = total vorticity (3), linear impulse (3), angular
 // impulse (3), enstrophy, helicity; out[11] = kinetic energy.
 size_t diag_scratch_doubles(int n);
-cudaError_t launch_diagnostics(int n, const double4 *pos64, const double4 *vor64,
+cudaError_t launch_diagnostics(int n, int kernel, const double4 *pos64, const double4 *vor64,
                                const int *wake_id, double *scratch, double *out, bool quadratic,
                                cudaStream_t s);
 
 // Vorticity field (FP64) of one system: field[3i..3i+2] = sum_j Z_ij alpha_j.
-cudaError_t launch_influence(int n, const double4 *pos64, const double4 *vor64, double *field,
-                             cudaStream_t s);
+cudaError_t launch_influence(int n, int kernel, const double4 *pos64, const double4 *vor64,
+                             double *field, cudaStream_t s);
 
 // Throughput probes: FP32 FFMA and FP64 DFMA chains.  flops = launched FMAs * 2.
 cudaError_t launch_ffma_peak(int blocks, int threads, int iters, float *sink, cudaStream_t s);

@@ -204,10 +204,10 @@ cudaError_t device_slot(int dev, DeviceSlot *out) {
     int sms = 0, bps = 0;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return e;
-    e = pairs_f32_occupancy(PairConfig{kNaTB, 1, 2}, true, &bps);
+    e = pairs_f32_occupancy(PairConfig{kNaTB, 1, 2}, true, KERNEL_HIGHORDER, &bps);
     if (e != cudaSuccess) return e;
     int bps0 = 0;
-    e = pairs_f32_occupancy(PairConfig{kNaTB, 1, 2}, false, &bps0);
+    e = pairs_f32_occupancy(PairConfig{kNaTB, 1, 2}, false, KERNEL_HIGHORDER, &bps0);
     if (e != cudaSuccess) return e;
     s.grid = sms * (bps < bps0 ? bps : bps0);
     s.scratch = static_cast<NoallocScratch *>(ptr);
@@ -238,7 +238,7 @@ extern "C" int pawan_interact_noalloc(const double *position, const double *vort
                                                      volume, ni);
   noalloc_plan<<<1, 256, 0, s>>>(slot.scratch, ni, pblocks, nu);
   const int items = ((ni + kNaTB - 1) / kNaTB) * ((ni + kNaChunk - 1) / kNaChunk);
-  cudaError_t e = launch_pairs_f32(PairConfig{kNaTB, 1, 2}, nu != 0.0, slot.grid,
+  cudaError_t e = launch_pairs_f32(PairConfig{kNaTB, 1, 2}, nu != 0.0, KERNEL_HIGHORDER, slot.grid,
                                    slot.scratch->items, items, &slot.scratch->seg,
                                    &slot.scratch->counter, s);
   if (e != cudaSuccess) return PAWAN_ERR_CUDA;

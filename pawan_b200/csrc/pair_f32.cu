@@ -165,11 +165,63 @@ __device__ __forceinline__ void kernel_scalars_uniform(float h, float c240, floa
   fs = fmaf(80.f, ds, -qs) * ri2;
 }
 
+// The Gaussian kernel (gaussian.h:20-59) in the units of kernel_scalars: with
+// x2 = rho^2/sigma^2, e = exp(-x2/2) and K = sqrt(2/pi),
+//   qh = gq / sigma^3,        gq = (erf(x/sqrt 2)/x - K e) / x2,
+//   fh = gf / (3 sigma^5),    gf = (K e - 3 gq) / x2,
+//   dp = (2/15) K e / sigma^5.
+// Below x2 = 1 the closed forms lose digits to cancellation; there gq and gf
+// come from their power series in y = -x2/2,
+//   gq = K sum_m y^m / (m! (2m+3)),   gf = -K sum_m y^m / (m! (2m+5)),
+// nine terms (relative truncation error < 1e-8 at x2 = 1).
+__device__ __forceinline__ void gauss_scalars(float sig2, float r2, float ri, float &qh, float &fh,
+                                              float &dp) {
+  const float K = 0.797884561f;
+  const float is = rsqrtf(sig2);
+  const float is2 = is * is;
+  const float is3 = is2 * is;
+  const float x2 = r2 * is2;
+  const float e = expf(-0.5f * x2);
+  float gq, gf;
+  if (x2 < 1.0f) {
+    const float y = -0.5f * x2;
+    float sq = 1.0f / (40320.0f * 19.0f), sf = 1.0f / (40320.0f * 21.0f);
+    sq = fmaf(sq, y, 1.0f / (5040.0f * 17.0f));
+    sf = fmaf(sf, y, 1.0f / (5040.0f * 19.0f));
+    sq = fmaf(sq, y, 1.0f / (720.0f * 15.0f));
+    sf = fmaf(sf, y, 1.0f / (720.0f * 17.0f));
+    sq = fmaf(sq, y, 1.0f / (120.0f * 13.0f));
+    sf = fmaf(sf, y, 1.0f / (120.0f * 15.0f));
+    sq = fmaf(sq, y, 1.0f / (24.0f * 11.0f));
+    sf = fmaf(sf, y, 1.0f / (24.0f * 13.0f));
+    sq = fmaf(sq, y, 1.0f / (6.0f * 9.0f));
+    sf = fmaf(sf, y, 1.0f / (6.0f * 11.0f));
+    sq = fmaf(sq, y, 1.0f / (2.0f * 7.0f));
+    sf = fmaf(sf, y, 1.0f / (2.0f * 9.0f));
+    sq = fmaf(sq, y, 1.0f / 5.0f);
+    sf = fmaf(sf, y, 1.0f / 7.0f);
+    sq = fmaf(sq, y, 1.0f / 3.0f);
+    sf = fmaf(sf, y, 1.0f / 5.0f);
+    gq = K * sq;
+    gf = -K * sf;
+  } else {
+    const float x = r2 * ri * is;  // rho / sigma
+    const float ix = rcp_approx(x);
+    const float ix2 = ix * ix;
+    gq = fmaf(erff(0.707106781f * x), ix, -K * e) * ix2;
+    gf = fmaf(-3.0f, gq, K * e) * ix2;
+  }
+  const float is5 = is3 * is2;
+  qh = gq * is3;
+  fh = gf * is5 * (1.0f / 3.0f);
+  dp = (2.0f / 15.0f) * K * e * is5;
+}
+
 // Far tile, shared-memory format (written when the tile is staged):
 //   sa[j] = (x'_j, h_j),  sb[j] = (alpha_j, v_j),  sc[j] = (beta_j, 0).
 // UNI: every pair has sigma^2 = 2 hu (sums in the units of
 // kernel_scalars_uniform).
-template <bool DIFF, bool UNI, int P, int R, int NSRC, int U>
+template <bool DIFF, bool UNI, int P, int R, int NSRC, int U, int KERN>
 __device__ __forceinline__ void tile_far(const float4 *__restrict__ sa,
                                          const float4 *__restrict__ sb,
                                          const float4 *__restrict__ sc, int g,
@@ -192,6 +244,8 @@ __device__ __forceinline__ void tile_far(const float4 *__restrict__ sa,
         const float w = rsqrtf(r2 + s2u);
         const float ri = rsqrtf(r2);
         kernel_scalars_uniform(hu, c240, w, ri, r2, qh, fh, dp);
+      } else if (KERN == KERNEL_GAUSSIAN) {
+        gauss_scalars(T[r].h + p.w, r2, rsqrtf(r2), qh, fh, dp);
       } else {
         const float sig2 = T[r].h + p.w;
         const float w = rsqrtf(r2 + sig2);
@@ -252,7 +306,7 @@ struct Target2 {
 
 __device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
 
-template <bool DIFF, bool UNI, bool RCP, int NSRC, int U>
+template <bool DIFF, bool UNI, bool RCP, int NSRC, int U, int KERN>
 __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
                                                 const float4 *__restrict__ f1,
                                                 const float4 *__restrict__ f2,
@@ -291,6 +345,15 @@ __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
       const float2 ph = __fmul2_rn(__ffma2_rn(u, y, y), ri);
       qh = __fmul2_rn(__ffma2_rn(c240, dp, ph), ri2);
       nfh = __fmul2_rn(__ffma2_rn(bc2(-80.f), dp, qh), ri2);
+    } else if (KERN == KERNEL_GAUSSIAN) {
+      // one source at a time (exp and erf do not pair), returning -fh
+      const float2 sig2 = __fadd2_rn(T.h, hj);
+      float qa, fa, da, qb, fb, db;
+      gauss_scalars(sig2.x, r2.x, rsqrtf(r2.x), qa, fa, da);
+      gauss_scalars(sig2.y, r2.y, rsqrtf(r2.y), qb, fb, db);
+      qh = make_float2(qa, qb);
+      nfh = make_float2(-fa, -fb);
+      dp = make_float2(da, db);
     } else {
       // kernel_scalars in pairs, returning -fh
       const float2 sig2 = __fadd2_rn(T.h, hj);
@@ -352,7 +415,7 @@ __device__ __forceinline__ void cross_accurate(float ax, float ay, float az, flo
 
 // Near tile, shared-memory format: sp, sv, spl, svl = pos32, vor32, poslo,
 // vorlo of the sources; tpl, tvl = poslo, vorlo of the targets.
-template <bool DIFF, bool CHECK, int P, int R, int NSRC>
+template <bool DIFF, bool CHECK, int P, int R, int NSRC, int KERN>
 __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
                                           const float4 *__restrict__ sv,
                                           const float4 *__restrict__ spl,
@@ -376,10 +439,14 @@ __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
       const float dz = (T[r].zh - p.z) + (tpl[r].z - pl.z);
       const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
       const float sig2 = T[r].h + p.w;
-      const float w = rsqrtf(r2 + sig2);
       const float ri = rsqrtf(r2);
       float qh, fh, dp;
-      kernel_scalars(sig2, w, ri, qh, fh, dp);
+      if (KERN == KERNEL_GAUSSIAN) {
+        gauss_scalars(sig2, r2, ri, qh, fh, dp);
+      } else {
+        const float w = rsqrtf(r2 + sig2);
+        kernel_scalars(sig2, w, ri, qh, fh, dp);
+      }
       // velocity: alpha_j x d
       const float cx = fmaf(s.y, dz, -s.z * dy);
       const float cy = fmaf(s.z, dx, -s.x * dz);
@@ -442,7 +509,9 @@ __device__ __forceinline__ bool far_tiles(float4 tlo, float4 thi, float4 slo, fl
 // 1), taking 1/rho^2 on uniform-radius tiles from the MUFU reciprocal (PK = 1)
 // or from rsqrt squared (PK = 2).
 // MINB: blocks per SM the register allocation is bounded for (occupancy).
-template <int TB, int P, int R, int U, bool DIFF, int MINB, int PK>
+// KERN: the smoothing kernel (SmoothingKernel); the uniform-radius
+// specialisation exists for the high-order kernel only.
+template <int TB, int P, int R, int U, bool DIFF, int MINB, int PK, int KERN>
 __global__ void __launch_bounds__(TB, MINB)
     pairs_f32_kernel(const WorkItem *__restrict__ items, int n_items,
                      const SegDesc *__restrict__ segs, int *__restrict__ next_item) {
@@ -524,7 +593,7 @@ __global__ void __launch_bounds__(TB, MINB)
       const bool diag = (ts < w.t0 + TPB) && (w.t0 < ts + TB);
       const bool near = diag || !far_tiles(tlo, thi, slo, shi, sg.near2);
       // one smoothing radius over both tiles
-      const bool uni = tlo.w == thi.w && slo.w == shi.w && tlo.w == slo.w;
+      const bool uni = KERN == KERNEL_HIGHORDER && tlo.w == thi.w && slo.w == shi.w && tlo.w == slo.w;
       const float cx = 0.5f * (slo.x + shi.x), cy = 0.5f * (slo.y + shi.y),
                   cz = 0.5f * (slo.z + shi.z);
       // this thread's own slot of the tile: wait for its copies, then rewrite
@@ -591,11 +660,11 @@ __global__ void __launch_bounds__(TB, MINB)
         b.wx = b.wy = b.wz = b.qx = b.qy = b.qz = b.gx = b.gy = b.gz = make_float2(0.f, 0.f);
         b.ex = b.ey = b.ez = b.ev = make_float2(0.f, 0.f);
         if (uni)
-          tile_far_packed<DIFF, true, PK == 1, TB, U>(fq + buf * FQ, fq + (2 + buf) * FQ,
+          tile_far_packed<DIFF, true, PK == 1, TB, U, KERN>(fq + buf * FQ, fq + (2 + buf) * FQ,
                                                       fq + (4 + buf) * FQ, fq + (6 + buf) * FQ,
                                                       fq + (8 + buf) * FQ, fz + buf * FQ, T2, slo.w, b);
         else
-          tile_far_packed<DIFF, false, PK == 1, TB, U>(fq + buf * FQ, fq + (2 + buf) * FQ,
+          tile_far_packed<DIFF, false, PK == 1, TB, U, KERN>(fq + buf * FQ, fq + (2 + buf) * FQ,
                                                        fq + (4 + buf) * FQ, fq + (6 + buf) * FQ,
                                                        fq + (8 + buf) * FQ, fz + buf * FQ, T2, 0.f, b);
         const double s2 = uni ? 2.0 * (double)slo.w : 1.0;
@@ -628,10 +697,10 @@ __global__ void __launch_bounds__(TB, MINB)
           F[r].gz = fmaf(F[r].x, T[r].bh, -F[r].y * T[r].ah);
         }
         if (uni)
-          tile_far<DIFF, true, P, R, TB, U>(sp + buf * TB, sv + buf * TB, spl + buf * TB, g, T, F,
+          tile_far<DIFF, true, P, R, TB, U, KERN>(sp + buf * TB, sv + buf * TB, spl + buf * TB, g, T, F,
                                             slo.w, a);
         else
-          tile_far<DIFF, false, P, R, TB, U>(sp + buf * TB, sv + buf * TB, spl + buf * TB, g, T, F,
+          tile_far<DIFF, false, P, R, TB, U, KERN>(sp + buf * TB, sv + buf * TB, spl + buf * TB, g, T, F,
                                              0.f, a);
         // undo the uniform-radius scaling: qh = sigma^2 qs, fh = sigma^2 fs, Dp = 32 ds
         const double s2 = uni ? 2.0 * (double)slo.w : 1.0;
@@ -665,10 +734,10 @@ __global__ void __launch_bounds__(TB, MINB)
           tvl[r] = valid[r] ? __ldg(sg.vorlo + ti[r]) : make_float4(0.f, 0.f, 0.f, 0.f);
         }
         if (diag)
-          tile_near<DIFF, true, P, R, TB>(sp + buf * TB, sv + buf * TB, spl + buf * TB,
+          tile_near<DIFF, true, P, R, TB, KERN>(sp + buf * TB, sv + buf * TB, spl + buf * TB,
                                           svl + buf * TB, g, skip, T, tpl, tvl, a);
         else
-          tile_near<DIFF, false, P, R, TB>(sp + buf * TB, sv + buf * TB, spl + buf * TB,
+          tile_near<DIFF, false, P, R, TB, KERN>(sp + buf * TB, sv + buf * TB, spl + buf * TB,
                                            svl + buf * TB, g, skip, T, tpl, tvl, a);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -719,11 +788,13 @@ __global__ void __launch_bounds__(TB, MINB)
 using KernelFn = void (*)(const WorkItem *, int, const SegDesc *, int *);
 
 template <bool DIFF>
-KernelFn select(const PairConfig &c) {
+KernelFn select_highorder(const PairConfig &c) {
 #define PAWAN_F32_CASE_PK(TB_, P_, R_, U_, MINB_, PK_)                                   \
+  PAWAN_F32_CASE_K(TB_, P_, R_, U_, MINB_, PK_, KERNEL_HIGHORDER)
+#define PAWAN_F32_CASE_K(TB_, P_, R_, U_, MINB_, PK_, KERN_)                             \
   if (c.tb == TB_ && c.p == P_ && c.r == R_ && c.unroll == U_ && c.packed == PK_ &&      \
       (c.minb == MINB_ || (c.minb == 0 && MINB_ == (TB_ <= 128 ? 4 : 2))))              \
-    return &pairs_f32_kernel<TB_, P_, R_, U_, DIFF, MINB_, PK_>;
+    return &pairs_f32_kernel<TB_, P_, R_, U_, DIFF, MINB_, PK_, KERN_>;
 #define PAWAN_F32_CASE(TB_, P_, R_, U_, MINB_) PAWAN_F32_CASE_PK(TB_, P_, R_, U_, MINB_, 0)
   PAWAN_F32_CASE_PK(128, 1, 1, 1, 4, 1)
   PAWAN_F32_CASE_PK(128, 1, 1, 2, 4, 1)
@@ -754,13 +825,27 @@ KernelFn select(const PairConfig &c) {
   PAWAN_F32_CASE(256, 1, 2, 1, 2)
   PAWAN_F32_CASE(256, 1, 2, 2, 2)
   PAWAN_F32_CASE(256, 1, 1, 4, 3)
-#undef PAWAN_F32_CASE
-#undef PAWAN_F32_CASE_PK
   return nullptr;
 }
 
-KernelFn select(const PairConfig &c, bool diffusion) {
-  return diffusion ? select<true>(c) : select<false>(c);
+// The Gaussian kernel is compiled for the default tilings only.
+template <bool DIFF>
+KernelFn select_gaussian(const PairConfig &c) {
+  PAWAN_F32_CASE_K(128, 1, 1, 4, 4, 1, KERNEL_GAUSSIAN)
+  PAWAN_F32_CASE_K(128, 1, 1, 2, 4, 0, KERNEL_GAUSSIAN)
+  PAWAN_F32_CASE_K(128, 2, 1, 4, 4, 0, KERNEL_GAUSSIAN)
+  PAWAN_F32_CASE_K(256, 1, 1, 4, 2, 1, KERNEL_GAUSSIAN)
+  return nullptr;
+}
+#undef PAWAN_F32_CASE
+#undef PAWAN_F32_CASE_PK
+#undef PAWAN_F32_CASE_K
+
+KernelFn select(const PairConfig &c, bool diffusion, int kernel) {
+  if (kernel == KERNEL_GAUSSIAN) return diffusion ? select_gaussian<true>(c) : select_gaussian<false>(c);
+  if (kernel == KERNEL_HIGHORDER)
+    return diffusion ? select_highorder<true>(c) : select_highorder<false>(c);
+  return nullptr;
 }
 
 // Dynamic shared memory of a tiling: the staged ring plus the packed far format.
@@ -786,10 +871,12 @@ cudaError_t prepare(KernelFn f, size_t bytes) {
 
 }  // namespace
 
-bool pairs_f32_supported(const PairConfig &c) { return select(c, true) != nullptr; }
+bool pairs_f32_supported(const PairConfig &c, int kernel) {
+  return select(c, true, kernel) != nullptr;
+}
 
-cudaError_t pairs_f32_occupancy(const PairConfig &c, bool diffusion, int *blocks_per_sm) {
-  KernelFn f = select(c, diffusion);
+cudaError_t pairs_f32_occupancy(const PairConfig &c, bool diffusion, int kernel, int *blocks_per_sm) {
+  KernelFn f = select(c, diffusion, kernel);
   if (!f) return cudaErrorInvalidValue;
   const size_t bytes = smem_bytes(c);
   cudaError_t e = prepare(f, bytes);
@@ -797,9 +884,10 @@ cudaError_t pairs_f32_occupancy(const PairConfig &c, bool diffusion, int *blocks
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, c.tb, bytes);
 }
 
-cudaError_t launch_pairs_f32(const PairConfig &c, bool diffusion, int grid, const WorkItem *items,
-                             int n_items, const SegDesc *segs, int *next_item, cudaStream_t s) {
-  KernelFn f = select(c, diffusion);
+cudaError_t launch_pairs_f32(const PairConfig &c, bool diffusion, int kernel, int grid,
+                             const WorkItem *items, int n_items, const SegDesc *segs,
+                             int *next_item, cudaStream_t s) {
+  KernelFn f = select(c, diffusion, kernel);
   if (!f) return cudaErrorInvalidValue;
   const size_t bytes = smem_bytes(c);
   cudaError_t e = prepare(f, bytes);

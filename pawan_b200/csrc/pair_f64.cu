@@ -7,7 +7,11 @@
 //
 // Reference: INTERACT (src/interaction/interaction_utils.h:363-407), KERNEL
 // (src/interaction/highorder.h:48-60), __interaction::interact
-// (src/interaction/interaction.cpp:95-108).
+// (src/interaction/interaction.cpp:95-108).  The Gaussian kernel
+// (src/interaction/gaussian.h:20-59) in the same units: with x2 = rho^2/sigma^2,
+// e = exp(-x2/2), K = sqrt(2/pi), gq = (erf(x/sqrt 2)/x - K e)/x2 and
+// gf = (K e - 3 gq)/x2: qh = gq/sigma^3, fh = gf/(3 sigma^5),
+// dp = (2/15) K e / sigma^5 (closed forms, as the reference evaluates them).
 #include "device.cuh"
 #include "kernels.h"
 
@@ -25,7 +29,23 @@ __device__ __forceinline__ void load_source_f64(const SegDesc &sg, int j, int s1
   }
 }
 
-template <int TB, bool DIFF>
+// Gaussian qh, fh, dp (see the file comment) from r2, sig2 and 1/rho.
+__device__ __forceinline__ void gauss_f64(double r2, double sig2, double ri, double &qh,
+                                          double &fh, double &dp) {
+  const double is = rsqrt(sig2);
+  const double is2 = is * is;
+  const double is3 = is2 * is;
+  const double x2 = r2 * is2;
+  const double e = exp(-0.5 * x2);
+  const double x = r2 * ri * is;
+  const double gq = (erf(kSqrtHalf * x) / x - kSqrt2OverPi * e) / x2;
+  const double gf = (kSqrt2OverPi * e - 3.0 * gq) / x2;
+  qh = gq * is3;
+  fh = gf * is3 * is2 / 3.0;
+  dp = (2.0 / 15.0) * kSqrt2OverPi * e * is3 * is2;
+}
+
+template <int TB, bool DIFF, int KERN>
 __global__ void __launch_bounds__(TB)
     pairs_f64_kernel(const WorkItem *__restrict__ items, int n_items,
                      const SegDesc *__restrict__ segs, int *__restrict__ next_item) {
@@ -73,19 +93,24 @@ __global__ void __launch_bounds__(TB)
         const double dx = pi.x - p.x, dy = pi.y - p.y, dz = pi.z - p.z;
         const double r2 = fma(dz, dz, fma(dy, dy, dx * dx));
         const double sig2 = fma(0.5 * p.w, p.w, hi);
-        const double wr = rsqrt(r2 + sig2);
         const double ri = rsqrt(r2);
-        const double ri2 = ri * ri;
-        const double w2 = wr * wr;
-        const double w4 = w2 * w2;
-        const double uu = sig2 * w2;
-        const double u2 = uu * uu;
-        const double u4 = u2 * u2;
-        double dp = u4 * uu * (w4 * wr);
-        const double zc = dp * sig2;
-        const double ph = fma(1.5, sig2, r2) * w4 * ri;
-        double qh = fma(-7.5, zc, ph) * sig2 * ri2;
-        const double fh = fma(2.5, zc, -qh) * ri2;
+        double qh, fh, dp;
+        if (KERN == KERNEL_GAUSSIAN) {
+          gauss_f64(r2, sig2, ri, qh, fh, dp);
+        } else {
+          const double wr = rsqrt(r2 + sig2);
+          const double ri2 = ri * ri;
+          const double w2 = wr * wr;
+          const double w4 = w2 * w2;
+          const double uu = sig2 * w2;
+          const double u2 = uu * uu;
+          const double u4 = u2 * u2;
+          dp = u4 * uu * (w4 * wr);
+          const double zc = dp * sig2;
+          const double ph = fma(1.5, sig2, r2) * w4 * ri;
+          qh = fma(-7.5, zc, ph) * sig2 * ri2;
+          fh = fma(2.5, zc, -qh) * ri2;
+        }
         const double cx = fma(s.y, dz, -s.z * dy);
         const double cy = fma(s.z, dx, -s.x * dz);
         const double cz = fma(s.x, dy, -s.y * dx);
@@ -140,26 +165,36 @@ __global__ void __launch_bounds__(TB)
 
 using KernelFn = void (*)(const WorkItem *, int, const SegDesc *, int *);
 
-KernelFn select(const PairConfig &c, bool diffusion) {
-  if (c.p != 1 || c.r != 1) return nullptr;
-  if (c.tb == 128) return diffusion ? &pairs_f64_kernel<128, true> : &pairs_f64_kernel<128, false>;
-  if (c.tb == 256) return diffusion ? &pairs_f64_kernel<256, true> : &pairs_f64_kernel<256, false>;
+template <int KERN>
+KernelFn select_k(const PairConfig &c, bool diffusion) {
+  if (c.tb == 128)
+    return diffusion ? &pairs_f64_kernel<128, true, KERN> : &pairs_f64_kernel<128, false, KERN>;
+  if (c.tb == 256)
+    return diffusion ? &pairs_f64_kernel<256, true, KERN> : &pairs_f64_kernel<256, false, KERN>;
+  return nullptr;
+}
+
+KernelFn select(const PairConfig &c, bool diffusion, int kernel) {
+  if (c.p != 1 || c.r != 1 || c.packed != 0) return nullptr;
+  if (kernel == KERNEL_GAUSSIAN) return select_k<KERNEL_GAUSSIAN>(c, diffusion);
+  if (kernel == KERNEL_HIGHORDER) return select_k<KERNEL_HIGHORDER>(c, diffusion);
   return nullptr;
 }
 
 }  // namespace
 
-bool pairs_f64_supported(const PairConfig &c) { return select(c, true) != nullptr; }
+bool pairs_f64_supported(const PairConfig &c, int kernel) { return select(c, true, kernel) != nullptr; }
 
-cudaError_t pairs_f64_occupancy(const PairConfig &c, bool diffusion, int *blocks_per_sm) {
-  KernelFn f = select(c, diffusion);
+cudaError_t pairs_f64_occupancy(const PairConfig &c, bool diffusion, int kernel, int *blocks_per_sm) {
+  KernelFn f = select(c, diffusion, kernel);
   if (!f) return cudaErrorInvalidValue;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, c.tb, 0);
 }
 
-cudaError_t launch_pairs_f64(const PairConfig &c, bool diffusion, int grid, const WorkItem *items,
-                             int n_items, const SegDesc *segs, int *next_item, cudaStream_t s) {
-  KernelFn f = select(c, diffusion);
+cudaError_t launch_pairs_f64(const PairConfig &c, bool diffusion, int kernel, int grid,
+                             const WorkItem *items, int n_items, const SegDesc *segs,
+                             int *next_item, cudaStream_t s) {
+  KernelFn f = select(c, diffusion, kernel);
   if (!f) return cudaErrorInvalidValue;
   f<<<grid, c.tb, 0, s>>>(items, n_items, segs, next_item);
   return cudaGetLastError();

@@ -16,14 +16,16 @@
 //   da = q (a_trg x a_src) + F [d.(a_trg x a_src)] d    :466, VORSTRETCH :69-100
 //   da += (Z nu / (sigma^2/2)) (v_trg a_src - v_src a_trg)   :467, DIFFUSION :253-286
 // written for target i (the reference's target role; the source role is the
-// same sum with d -> -d, see pair_f32.cu).
+// same sum with d -> -d, see pair_f32.cu).  With the Gaussian kernel
+// (gaussian.h:20-59): Z = exp(-rho_bar^2/2)/pow(sigma,3)/pow(2 pi,1.5),
+// phi = 0.25/pi erf(rho_bar/sqrt 2)/sigma^3, q and F as above.
 #include "device.cuh"
 #include "kernels.h"
 
 namespace pawan {
 namespace {
 
-template <int TB>
+template <int TB, int KERN>
 __global__ void __launch_bounds__(TB)
     pairs_plain_kernel(const WorkItem *__restrict__ items, int n_items,
                        const SegDesc *__restrict__ segs, int *__restrict__ next_item) {
@@ -71,11 +73,16 @@ __global__ void __launch_bounds__(TB)
         const double sigma = sqrt(0.5 * (p.w * p.w + pi.w * pi.w));
         // KERNEL
         const double rho_bar = rho / sigma;
-        const double Z =
-            1.875 * one_over_pi / pow(rho_bar * rho_bar + 1.0, 7.5) / pow(sigma, 3.0);
         const double rho_bar2 = rho_bar * rho_bar;
         const double sig3 = sigma * sigma * sigma;
-        const double phi = 0.25 * one_over_pi * (rho_bar2 + 1.5) / pow(rho_bar2 + 1.0, 2.0) / sig3;
+        double Z, phi;
+        if (KERN == KERNEL_GAUSSIAN) {
+          Z = exp(-0.5 * rho_bar * rho_bar) / pow(sigma, 3.0) / pow(2.0 * kPi, 1.5);
+          phi = 0.25 * one_over_pi * erf(kSqrtHalf * rho_bar) / sig3;
+        } else {
+          Z = 1.875 * one_over_pi / pow(rho_bar * rho_bar + 1.0, 7.5) / pow(sigma, 3.0);
+          phi = 0.25 * one_over_pi * (rho_bar2 + 1.5) / pow(rho_bar2 + 1.0, 2.0) / sig3;
+        }
         const double q = (phi / rho_bar - Z) / rho_bar2;
         const double F = (Z - 3.0 * q) / (rho * rho);
         // VELOCITY: q (alpha_src x d)
@@ -111,26 +118,28 @@ __global__ void __launch_bounds__(TB)
 
 using KernelFn = void (*)(const WorkItem *, int, const SegDesc *, int *);
 
-KernelFn select(const PairConfig &c) {
-  if (c.p != 1 || c.r != 1) return nullptr;
-  if (c.tb == 128) return &pairs_plain_kernel<128>;
-  if (c.tb == 256) return &pairs_plain_kernel<256>;
+KernelFn select(const PairConfig &c, int kernel) {
+  if (c.p != 1 || c.r != 1 || c.packed != 0) return nullptr;
+  const bool g = kernel == KERNEL_GAUSSIAN;
+  if (kernel != KERNEL_HIGHORDER && !g) return nullptr;
+  if (c.tb == 128) return g ? &pairs_plain_kernel<128, 1> : &pairs_plain_kernel<128, 0>;
+  if (c.tb == 256) return g ? &pairs_plain_kernel<256, 1> : &pairs_plain_kernel<256, 0>;
   return nullptr;
 }
 
 }  // namespace
 
-bool pairs_plain_supported(const PairConfig &c) { return select(c) != nullptr; }
+bool pairs_plain_supported(const PairConfig &c, int kernel) { return select(c, kernel) != nullptr; }
 
-cudaError_t pairs_plain_occupancy(const PairConfig &c, int *blocks_per_sm) {
-  KernelFn f = select(c);
+cudaError_t pairs_plain_occupancy(const PairConfig &c, int kernel, int *blocks_per_sm) {
+  KernelFn f = select(c, kernel);
   if (!f) return cudaErrorInvalidValue;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, c.tb, 0);
 }
 
-cudaError_t launch_pairs_plain(const PairConfig &c, int grid, const WorkItem *items, int n_items,
-                               const SegDesc *segs, int *next_item, cudaStream_t s) {
-  KernelFn f = select(c);
+cudaError_t launch_pairs_plain(const PairConfig &c, int kernel, int grid, const WorkItem *items,
+                               int n_items, const SegDesc *segs, int *next_item, cudaStream_t s) {
+  KernelFn f = select(c, kernel);
   if (!f) return cudaErrorInvalidValue;
   f<<<grid, c.tb, 0, s>>>(items, n_items, segs, next_item);
   return cudaGetLastError();

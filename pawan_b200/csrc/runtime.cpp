@@ -50,7 +50,7 @@ TileChoice default_tile(int precision) {
   return t;
 }
 
-std::vector<TileChoice> tile_candidates(int precision) {
+std::vector<TileChoice> tile_candidates(int precision, int kernel) {
   std::vector<TileChoice> v;
   if (precision == PAWAN_PREC_F32) {
     // (threads per target, targets per thread, unroll, blocks per SM) as
@@ -65,7 +65,7 @@ std::vector<TileChoice> tile_candidates(int precision) {
       for (const auto &sh : shapes) {
         TileChoice t;
         t.pc = PairConfig{tb, sh[0], sh[2], sh[1], sh[3], sh[4]};
-        if (pairs_f32_supported(t.pc)) v.push_back(t);
+        if (pairs_f32_supported(t.pc, kernel)) v.push_back(t);
       }
   } else {
     for (int tb : {128, 256}) {
@@ -90,24 +90,27 @@ bool Plan::stale() const {
 }
 
 static int occupancy(pawan_ctx *ctx, int precision, const PairConfig &pc, bool diffusion,
-                     int *bps) {
+                     int kernel, int *bps) {
   cudaError_t e;
   if (precision == PAWAN_PREC_F32)
-    e = pairs_f32_occupancy(pc, diffusion, bps);
+    e = pairs_f32_occupancy(pc, diffusion, kernel, bps);
   else if (precision == PAWAN_PREC_F64)
-    e = pairs_f64_occupancy(pc, diffusion, bps);
+    e = pairs_f64_occupancy(pc, diffusion, kernel, bps);
   else
-    e = pairs_plain_occupancy(pc, bps);
+    e = pairs_plain_occupancy(pc, kernel, bps);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "occupancy query");
   if (*bps < 1) return fail(ctx, PAWAN_ERR_INVALID, "pair kernel does not fit on an SM");
   return PAWAN_OK;
 }
 
-static bool tile_supported(int precision, const PairConfig &pc) {
-  if (precision == PAWAN_PREC_F32) return pairs_f32_supported(pc);
-  if (precision == PAWAN_PREC_F64) return pairs_f64_supported(pc);
-  return pairs_plain_supported(pc);
+static bool tile_supported(int precision, const PairConfig &pc, int kernel) {
+  if (precision == PAWAN_PREC_F32) return pairs_f32_supported(pc, kernel);
+  if (precision == PAWAN_PREC_F64) return pairs_f64_supported(pc, kernel);
+  return pairs_plain_supported(pc, kernel);
 }
+
+static_assert(PAWAN_KERNEL_HIGHORDER == KERNEL_HIGHORDER && PAWAN_KERNEL_GAUSSIAN == KERNEL_GAUSSIAN,
+              "public and device smoothing-kernel codes agree");
 
 // Process blocks of a sharded system start at multiples of kShardAlign
 // particles: whole stage blocks and whole target tiles of every tiling.
@@ -129,11 +132,16 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
                const TileChoice &tile, std::unique_ptr<Plan> &out, int fixed_chunk_sources,
                bool ordered_alloc) {
   if (systems.empty()) return fail(ctx, PAWAN_ERR_INVALID, "plan over no systems");
-  if (!tile_supported(precision, tile.pc))
-    return fail(ctx, PAWAN_ERR_INVALID, "unsupported pair tiling for this precision");
+  const int kernel = systems[0]->kernel;
+  for (auto *s : systems)
+    if (s->kernel != kernel)
+      return fail(ctx, PAWAN_ERR_INVALID, "systems of one plan must share the smoothing kernel");
+  if (!tile_supported(precision, tile.pc, kernel))
+    return fail(ctx, PAWAN_ERR_INVALID, "unsupported pair tiling for this precision and kernel");
   std::unique_ptr<Plan> p(new Plan());
   p->systems = systems;
   p->precision = precision;
+  p->kernel = kernel;
   p->tile = tile;
   for (auto *s : systems) {
     p->nus.push_back(s->nu);
@@ -144,7 +152,7 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     p->interactions += targets * (double)s->n;
   }
   int bps = 0;
-  PAWAN_TRY(occupancy(ctx, precision, tile.pc, p->diffusion, &bps));
+  PAWAN_TRY(occupancy(ctx, precision, tile.pc, p->diffusion, kernel, &bps));
   p->grid = ctx->sm_count * bps;
   const int TB = tile.pc.tb;
   const int TPB = targets_per_block(tile.pc);
@@ -335,13 +343,13 @@ int launch_pairs(pawan_ctx *ctx, Plan &p, bool allow_events) {
   }
   cudaError_t e;
   if (p.precision == PAWAN_PREC_F32)
-    e = launch_pairs_f32(p.tile.pc, p.diffusion, p.grid, p.items.p, p.n_items, p.segs.p,
+    e = launch_pairs_f32(p.tile.pc, p.diffusion, p.kernel, p.grid, p.items.p, p.n_items, p.segs.p,
                          ctx->d_counter, ctx->stream);
   else if (p.precision == PAWAN_PREC_F64)
-    e = launch_pairs_f64(p.tile.pc, p.diffusion, p.grid, p.items.p, p.n_items, p.segs.p,
+    e = launch_pairs_f64(p.tile.pc, p.diffusion, p.kernel, p.grid, p.items.p, p.n_items, p.segs.p,
                          ctx->d_counter, ctx->stream);
   else
-    e = launch_pairs_plain(p.tile.pc, p.grid, p.items.p, p.n_items, p.segs.p, ctx->d_counter,
+    e = launch_pairs_plain(p.tile.pc, p.kernel, p.grid, p.items.p, p.n_items, p.segs.p, ctx->d_counter,
                            ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "pair kernel launch");
   ctx->launches++;
@@ -439,7 +447,7 @@ int autotune_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, in
     return PAWAN_OK;
   };
   // 1) tile shape at the default chunking, 2) chunking for the best shape.
-  for (const TileChoice &t : tile_candidates(precision)) {
+  for (const TileChoice &t : tile_candidates(precision, systems[0]->kernel)) {
     double ms = 0;
     status = time_tile(t, &ms);
     if (status != PAWAN_OK) break;
@@ -911,7 +919,7 @@ int pawan_system_euler(pawan_system *sys, double dt, size_t nsteps) {
 static int run_diagnostics(pawan_system *sys, bool quadratic, double *out12) {
   pawan_ctx *ctx = sys->ctx;
   if (!sys->has_particles) return fail(ctx, PAWAN_ERR_STATE, "particles not set");
-  cudaError_t e = launch_diagnostics((int)sys->n, sys->pos64.p, sys->vor64.p, sys->wake_id.p,
+  cudaError_t e = launch_diagnostics((int)sys->n, sys->kernel, sys->pos64.p, sys->vor64.p, sys->wake_id.p,
                                      sys->diag_scratch.p, sys->diag_out.p, quadratic, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "diagnostics launch");
   ctx->launches += quadratic ? 4 : 2;
@@ -948,7 +956,8 @@ int pawan_system_influence(pawan_system *sys, double *field, size_t size) {
   if (!sys->has_particles) return fail(ctx, PAWAN_ERR_STATE, "particles not set");
   if (!sys->field.p) PAWAN_CUDA(ctx, sys->field.alloc(3 * sys->n));
   // pos64 / vor64 hold pack(X) between API calls
-  PAWAN_CUDA(ctx, launch_influence((int)sys->n, sys->pos64.p, sys->vor64.p, sys->field.p, ctx->stream));
+  PAWAN_CUDA(ctx, launch_influence((int)sys->n, sys->kernel, sys->pos64.p, sys->vor64.p, sys->field.p,
+                                   ctx->stream));
   ctx->launches++;
   PAWAN_CUDA(ctx, cudaMemcpyAsync(field, sys->field.p, 3 * sys->n * sizeof(double),
                                   cudaMemcpyDeviceToHost, ctx->stream));
@@ -1026,6 +1035,28 @@ int pawan_ctx_stream(pawan_ctx *ctx, void **stream) {
   return PAWAN_OK;
 }
 
+int pawan_system_set_kernel(pawan_system *sys, int kernel) {
+  CHECK_SYS(sys);
+  if (kernel != PAWAN_KERNEL_HIGHORDER && kernel != PAWAN_KERNEL_GAUSSIAN)
+    return fail(sys->ctx, PAWAN_ERR_INVALID, "unknown smoothing kernel");
+  if (kernel != sys->kernel) {
+    sys->kernel = kernel;
+    if (!tile_supported(sys->precision, sys->tile.pc, kernel)) {
+      sys->tile = default_tile(sys->precision);
+      sys->fixed_tile = false;
+    }
+    sys->plan.reset();
+  }
+  return PAWAN_OK;
+}
+
+int pawan_system_get_kernel(pawan_system *sys, int *kernel) {
+  CHECK_SYS(sys);
+  if (!kernel) return PAWAN_ERR_INVALID;
+  *kernel = sys->kernel;
+  return PAWAN_OK;
+}
+
 int pawan_system_set_nu(pawan_system *sys, double nu) {
   CHECK_SYS(sys);
   if (!std::isfinite(nu) || nu < 0.0) return fail(sys->ctx, PAWAN_ERR_INVALID, "nu must be >= 0");
@@ -1039,7 +1070,7 @@ int pawan_system_set_precision(pawan_system *sys, int precision) {
     return fail(sys->ctx, PAWAN_ERR_INVALID, "unknown precision");
   if (precision != sys->precision) {
     sys->precision = precision;
-    if (!sys->fixed_tile || !tile_supported(precision, sys->tile.pc))
+    if (!sys->fixed_tile || !tile_supported(precision, sys->tile.pc, sys->kernel))
       sys->tile = default_tile(precision);
   }
   return PAWAN_OK;
@@ -1071,15 +1102,16 @@ int pawan_system_write_frame(pawan_system *sys, const char *path, double t, int 
   return PAWAN_OK;
 }
 
-static int tile_from_abi(pawan_ctx *ctx, int precision, const pawan_tiling *t, TileChoice *out) {
+static int tile_from_abi(pawan_ctx *ctx, int precision, int kernel, const pawan_tiling *t,
+                         TileChoice *out) {
   if (!t) return fail(ctx, PAWAN_ERR_INVALID, "null tiling");
   TileChoice c;
   c.pc = PairConfig{t->threads, t->threads_per_target, t->unroll, t->targets_per_thread,
                     t->blocks_per_sm, t->packed};
   c.items_per_slot = t->items_per_slot;
   if (t->items_per_slot < 1 || t->targets_per_thread < 1 || t->blocks_per_sm < 0 || t->packed < 0 ||
-      !tile_supported(precision, c.pc))
-    return fail(ctx, PAWAN_ERR_INVALID, "tiling not compiled for this precision");
+      !tile_supported(precision, c.pc, kernel))
+    return fail(ctx, PAWAN_ERR_INVALID, "tiling not compiled for this precision and kernel");
   *out = c;
   return PAWAN_OK;
 }
@@ -1087,7 +1119,7 @@ static int tile_from_abi(pawan_ctx *ctx, int precision, const pawan_tiling *t, T
 int pawan_system_set_tiling(pawan_system *sys, const pawan_tiling *tiling) {
   CHECK_SYS(sys);
   TileChoice t;
-  PAWAN_TRY(tile_from_abi(sys->ctx, sys->precision, tiling, &t));
+  PAWAN_TRY(tile_from_abi(sys->ctx, sys->precision, sys->kernel, tiling, &t));
   sys->tile = t;
   sys->fixed_tile = true;
   return PAWAN_OK;
@@ -1177,6 +1209,8 @@ int pawan_batch_create(pawan_ctx *ctx, size_t n, pawan_system *const *systems, p
       return fail(ctx, PAWAN_ERR_INVALID, "batch systems must share one precision");
     if (systems[i]->shard.active)
       return fail(ctx, PAWAN_ERR_INVALID, "a sharded system cannot join a batch");
+    if (systems[i]->kernel != systems[0]->kernel)
+      return fail(ctx, PAWAN_ERR_INVALID, "batch systems must share one smoothing kernel");
     b->systems.push_back(systems[i]);
   }
   b->tile = default_tile(b->precision);
@@ -1206,7 +1240,7 @@ int pawan_batch_solve(pawan_batch *b) {
 int pawan_batch_set_tiling(pawan_batch *b, const pawan_tiling *tiling) {
   if (!b) return PAWAN_ERR_INVALID;
   TileChoice t;
-  PAWAN_TRY(tile_from_abi(b->ctx, b->precision, tiling, &t));
+  PAWAN_TRY(tile_from_abi(b->ctx, b->precision, b->systems[0]->kernel, tiling, &t));
   b->tile = t;
   return PAWAN_OK;
 }

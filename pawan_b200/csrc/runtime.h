@@ -73,7 +73,7 @@ struct TileChoice {
 };
 
 TileChoice default_tile(int precision);
-std::vector<TileChoice> tile_candidates(int precision);
+std::vector<TileChoice> tile_candidates(int precision, int kernel);
 
 struct Plan;
 
@@ -109,6 +109,7 @@ struct pawan_system {
   size_t n = 0;
   double nu = 0.0;
   int precision = PAWAN_PREC_F32;
+  int kernel = PAWAN_KERNEL_HIGHORDER;  // smoothing kernel (SmoothingKernel)
   bool has_particles = false;
   bool fixed_tile = false;
   pawan::TileChoice tile;
@@ -148,6 +149,7 @@ struct Plan {
   std::vector<unsigned long long> geometry_versions;
   std::vector<unsigned long long> box_versions;  // pack_version the boxes were made at
   int precision = PAWAN_PREC_F32;
+  int kernel = PAWAN_KERNEL_HIGHORDER;
   TileChoice tile;
   bool diffusion = false;
   int grid = 0;

@@ -45,6 +45,11 @@ void __cuda::setViscosity(double nu) {
   if (_sys) check(pawan_system_set_nu(_sys, nu), "set_nu");
 }
 
+void __cuda::setKernel(int kernel) {
+  _kernel = kernel;
+  if (_sys) check(pawan_system_set_kernel(_sys, kernel), "set_kernel");
+}
+
 void __cuda::ensure_system() {
   if (!_ctx) check(pawan_ctx_create(_device, &_ctx), "context");
   if (_sys) return;
@@ -52,6 +57,7 @@ void __cuda::ensure_system() {
   for (auto *w : _wakes) counts.push_back(w->_numParticles);
   check(pawan_system_create(_ctx, counts.size(), counts.data(), _nu, _precision, &_sys),
         "system_create");
+  check(pawan_system_set_kernel(_sys, _kernel), "set_kernel");
 }
 
 // The wakes' matrices are row-major N x 3 (wake.cpp:10-21); copy rows so a

@@ -46,6 +46,10 @@ class __cuda : public __interaction {
 
   double kineticEnergy();
   void setViscosity(double nu);
+  /* The smoothing kernel the reference selects at compile time
+   * (interaction_utils.h:13-24): PAWAN_KERNEL_HIGHORDER (its default) or
+   * PAWAN_KERNEL_GAUSSIAN (src/interaction/gaussian.h). */
+  void setKernel(int kernel);
   /* Uploads the wakes' current positions and vorticities (and, the first time
    * or after addWake, radii and volumes). */
   void upload();
@@ -68,6 +72,7 @@ class __cuda : public __interaction {
   pawan_system *_sys = nullptr;
   int _precision;
   int _device;
+  int _kernel = PAWAN_KERNEL_HIGHORDER;
   bool _particles_uploaded = false;
   void ensure_system();
   void check(int status, const char *what) const;

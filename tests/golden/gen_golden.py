@@ -20,6 +20,9 @@ Cases (all FP64, reference layout for states/rates):
   vring1_influence   the same on the reference's __vring(1.0, 0.1, 1) (855
                      particles) with seeded layer strengths
   vring1_resolve     __resolve::rebuild on __vring(1.0, 0.1, 1): resolved strengths
+  pair64_gauss       the coaxial pair with the reference's Gaussian kernel
+                     (gaussian.h, compiled in by oracle/Makefile): solve, 2 RK4
+                     steps, diagnose, vorticity field
 """
 from __future__ import annotations
 
@@ -123,6 +126,18 @@ def main(only=()):
     _save("vring1_resolve", radius=np.float64(1.0), core=np.float64(0.1), layers=np.int64(1),
           pos=pos, rad=rad, vol=vol, strengths=resolved)
     v.close()
+
+    d = _inputs(pair)
+    ref = oracle.RefSystem(pair.counts, d["pos"], d["vor"], d["rad"], d["vol"], pair.nu, kernel="gaussian")
+    ref.solve()
+    rates = ref.get_rates()
+    diag = ref.diagnose()
+    field = ref.influence()
+    final = ref.rk4(d["state"], 0.005, 2)
+    _save("pair64_gauss", rates=rates, final_state=final, dt=np.float64(0.005), nsteps=np.int64(2),
+          total_vorticity=diag["total_vorticity"], linear_impulse=diag["linear_impulse"],
+          enstrophy=np.float64(diag["enstrophy"]), helicity=np.float64(diag["helicity"]),
+          field=field, **d)
 
 
 if __name__ == "__main__":

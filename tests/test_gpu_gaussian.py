@@ -1,0 +1,88 @@
+"""The reference's Gaussian smoothing kernel (src/interaction/gaussian.h) on
+the GPU, against the reference compiled with it (golden fixtures) and the
+oracle restatement: every precision, near and far tiles, mixed radii, RK4,
+diagnostics, the vorticity field.  Tolerances as for the default kernel."""
+import numpy as np
+import pytest
+
+import oracle
+from pawan_b200 import System, state_to_union, union_to_state
+from pawan_b200 import geometry as g
+from helpers import load, max_rel, rms_rel, split_rates, tol
+
+pytestmark = pytest.mark.gpu
+
+
+def check(prec, u, da, u_ref, da_ref):
+    t_rms, t_max = tol(prec)
+    assert rms_rel(u, u_ref) <= t_rms and rms_rel(da, da_ref) <= t_rms, (rms_rel(u, u_ref), rms_rel(da, da_ref))
+    assert max_rel(u, u_ref) <= t_max and max_rel(da, da_ref) <= t_max, (max_rel(u, u_ref), max_rel(da, da_ref))
+
+
+def gauss_system(ctx, counts, pos, vor, rad, vol, nu, prec):
+    s = System(ctx, counts, nu, prec)
+    s.set_kernel("gaussian")
+    s.set_particles(pos, vor, rad, vol)
+    assert s.kernel == "gaussian"
+    return s
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64", "f64_plain"])
+def test_gaussian_matches_golden(ctx, prec):
+    d = load("pair64_gauss")
+    counts = [int(c) for c in d["counts"]]
+    s = gauss_system(ctx, counts, d["pos"], d["vor"], d["rad"], d["vol"], float(d["nu"]), prec)
+    s.solve()
+    u_ref, da_ref = split_rates(counts, d["rates"])
+    check(prec, *s.union_rates(), u_ref, da_ref)
+    s.rk4(float(d["dt"]), int(d["nsteps"]))
+    inc = s.get_states() - d["state"]
+    assert rms_rel(inc, d["final_state"] - d["state"]) <= (1e-5 if prec == "f32" else 1e-10)
+    s.set_states(d["state"])
+    diag = s.diagnose()
+    assert diag["enstrophy"] == 0.0
+    assert abs(diag["helicity"] - d["helicity"]) <= 1e-10 * abs(d["helicity"])
+    k = s.influence()
+    assert rms_rel(k, d["field"]) <= 1e-12
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64", "f64_plain"])
+def test_gaussian_mixed_radii_near_and_far(ctx, prec):
+    sc = g.helical_wake(n_stations=64, seed=81, filaments=4, turns=2.0, nu=1e-3)  # N = 2,048
+    pos, vor, rad, vol = sc.union()
+    rad = rad * np.random.default_rng(8).uniform(0.7, 1.4, rad.shape)
+    s = gauss_system(ctx, sc.counts, pos, vor, rad, vol, sc.nu, prec)
+    s.solve()
+    check(prec, *s.union_rates(), *oracle.pairs(pos, vor, rad, vol, sc.nu, kernel="gaussian"))
+
+
+@pytest.mark.parametrize("tiling", [(128, 1, 1, 4, 0, 1), (128, 1, 1, 2, 0, 0), (128, 2, 1, 4, 0, 0),
+                                    (256, 1, 1, 4, 0, 1)])
+def test_gaussian_every_compiled_tiling(ctx, tiling):
+    sc = g.ring_pair(n_stations=70, seed=82, nu=1e-3)  # N = 1,120
+    pos, vor, rad, vol = sc.union()
+    u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, sc.nu, kernel="gaussian")
+    s = gauss_system(ctx, sc.counts, pos, vor, rad, vol, sc.nu, "f32")
+    tb, p, r, unroll, minb, packed = tiling
+    for ips in (1, 16):
+        s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=packed)
+        s.solve()
+        check("f32", *s.union_rates(), u_ref, da_ref)
+    s.autotune()  # only the tilings compiled for this kernel are candidates
+    s.solve()
+    check("f32", *s.union_rates(), u_ref, da_ref)
+
+
+def test_gaussian_rk4_matches_oracle_and_switching_back(ctx):
+    sc = g.single_ring(n_stations=64, seed=83, nu=2e-3)
+    pos, vor, rad, vol = sc.union()
+    s = gauss_system(ctx, sc.counts, pos, vor, rad, vol, sc.nu, "f32")
+    s.rk4(sc.dt, 3)
+    p1, v1 = oracle.rk4_step(pos, vor, rad, vol, sc.nu, sc.dt, 3, kernel="gaussian")
+    ref = union_to_state(sc.counts, p1, v1)
+    st0 = sc.state()
+    assert rms_rel(s.get_states() - st0, ref - st0) <= 1e-5
+    s.set_kernel("highorder")
+    s.set_states(st0)
+    s.solve()
+    check("f32", *s.union_rates(), *oracle.pairs(pos, vor, rad, vol, sc.nu))

@@ -158,3 +158,34 @@ def test_reference_vring_resolve_reproduces_golden():
             os.chdir(cwd)
     v.close()
     assert np.array_equal(s, d["strengths"])
+
+
+def test_restatement_matches_golden_gaussian_kernel():
+    """The reference compiled with its Gaussian kernel (gaussian.h): rates, two
+    RK4 steps, helicity (enstrophy is the reference's stub 0) and the field."""
+    d = load("pair64_gauss")
+    args = (d["pos"], d["vor"], d["rad"], d["vol"])
+    u_ref, da_ref = split_rates(d["counts"], d["rates"])
+    u, da = oracle.pairs(*args, float(d["nu"]), kernel="gaussian")
+    assert rms_rel(u, u_ref) < 1e-13 and rms_rel(da, da_ref) < 1e-13
+    p, v = oracle.rk4_step(*args, float(d["nu"]), float(d["dt"]), int(d["nsteps"]), kernel="gaussian")
+    out = union_to_state(list(d["counts"]), p, v)
+    assert rms_rel(out - d["state"], d["final_state"] - d["state"]) < 1e-11
+    assert float(d["enstrophy"]) == 0.0
+    assert oracle.enstrophy(d["pos"], d["vor"], d["rad"], kernel="gaussian") == 0.0
+    h = oracle.helicity(d["pos"], d["vor"], d["rad"], kernel="gaussian")
+    assert abs(h - d["helicity"]) <= 1e-11 * abs(d["helicity"]) + 1e-18
+    k = oracle.influence(d["pos"], d["vor"], d["rad"], kernel="gaussian")
+    assert rms_rel(k, d["field"]) < 1e-13
+
+
+@needs_ref
+def test_gaussian_reference_differs_from_default_kernel():
+    """The two compiled references really run different kernels."""
+    sc = g.ring_pair(n_stations=6, seed=19, nu=1e-3)
+    pos, vor, rad, vol = sc.union()
+    a = oracle.RefSystem(sc.counts, pos, vor, rad, vol, sc.nu)
+    b = oracle.RefSystem(sc.counts, pos, vor, rad, vol, sc.nu, kernel="gaussian")
+    a.solve()
+    b.solve()
+    assert rms_rel(a.get_rates(), b.get_rates()) > 1e-3
