@@ -50,6 +50,10 @@
 //    the pair loop for the per-tile fold (kernel_scalars_uniform).
 //    39 FP32 instructions per pair with one radius (43 with several; 4 fewer
 //    without diffusion).
+//  * far tiles whose every pair is at least 6 smoothing radii apart (box gap
+//    >= 6 sigma_max): the far formulation without the Z terms, which are below
+//    3e-9 of the terms they are added to there (kernel_scalars_nz); 29 FP32
+//    instructions per pair with one radius, no diffusion sums.
 // After each tile both are folded into six FP64 sums (u, dalpha) with the
 // target's strength in FP64 (hi + lo).
 //
@@ -165,6 +169,28 @@ __device__ __forceinline__ void kernel_scalars_uniform(float h, float c240, floa
   fs = fmaf(80.f, ds, -qs) * ri2;
 }
 
+// Far field without the Z terms.  Where every pair of a tile pair has
+// rho >= 6 sigma (checked on the tiles' boxes), Z = (15/8pi) sigma^-3
+// (rho_bar^2 + 1)^-7.5 is below 3e-9 of phi/rho_bar in q = (phi/rho_bar - Z)
+// / rho_bar^2 and of 3q in F = (Z - 3q)/rho^2, i.e. twenty times below FP32
+// rounding, and the diffusion rate 2 nu Z / sigma^2 (v_i alpha_j - v_j alpha_i)
+// of those pairs is as small against the near-field diffusion: the terms are
+// zero at FP32 resolution and are not formed.  What remains, with
+// y = 1/(rho^2 + sigma^2) and (rho^2 + 1.5 sigma^2) w^4 = y (1 + y sigma^2/2):
+//   qh = y (1 + y sigma^2/2) sigma^2 / rho^3,   fh = -qh / rho^2.
+// kernel_scalars_nz returns them for one sigma^2 per pair (12 FP32
+// instructions with the MUFU reciprocal and rsqrt); the uniform-radius form
+// returns qs = qh / sigma^2, -fs = qh / (sigma^2 rho^2) (8 instructions).
+__device__ __forceinline__ void kernel_scalars_nz(float sig2, float r2, float &qh, float &nfh) {
+  const float y = rcp_approx(r2 + sig2);
+  const float ri = rsqrtf(r2);
+  const float ri2 = ri * ri;
+  const float hy = 0.5f * sig2 * y;
+  const float ph = fmaf(hy, y, y);
+  qh = ph * sig2 * ri * ri2;
+  nfh = qh * ri2;
+}
+
 // The Gaussian kernel (gaussian.h:20-59) in the units of kernel_scalars: with
 // x2 = rho^2/sigma^2, e = exp(-x2/2) and K = sqrt(2/pi),
 //   qh = gq / sigma^3,        gq = (erf(x/sqrt 2)/x - K e) / x2,
@@ -221,7 +247,7 @@ __device__ __forceinline__ void gauss_scalars(float sig2, float r2, float ri, fl
 //   sa[j] = (x'_j, h_j),  sb[j] = (alpha_j, v_j),  sc[j] = (beta_j, 0).
 // UNI: every pair has sigma^2 = 2 hu (sums in the units of
 // kernel_scalars_uniform).
-template <bool DIFF, bool UNI, int P, int R, int NSRC, int U, int KERN>
+template <bool DIFF, bool UNI, int P, int R, int NSRC, int U, int KERN, bool NZ>
 __device__ __forceinline__ void tile_far(const float4 *__restrict__ sa,
                                          const float4 *__restrict__ sb,
                                          const float4 *__restrict__ sc, int g,
@@ -240,7 +266,21 @@ __device__ __forceinline__ void tile_far(const float4 *__restrict__ sa,
       const float dx = F[r].x - p.x, dy = F[r].y - p.y, dz = F[r].z - p.z;
       const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
       float qh, fh, dp;
-      if (UNI) {
+      if (NZ) {
+        // Z-free far field (kernel_scalars_nz); the diffusion sums stay 0
+        float nfh;
+        if (UNI) {
+          const float y = rcp_approx(r2 + s2u);
+          const float ri = rsqrtf(r2);
+          const float ri2 = ri * ri;
+          qh = fmaf(hu * y, y, y) * ri * ri2;
+          nfh = qh * ri2;
+        } else {
+          kernel_scalars_nz(T[r].h + p.w, r2, qh, nfh);
+        }
+        fh = -nfh;
+        dp = 0.f;
+      } else if (UNI) {
         const float w = rsqrtf(r2 + s2u);
         const float ri = rsqrtf(r2);
         kernel_scalars_uniform(hu, c240, w, ri, r2, qh, fh, dp);
@@ -265,7 +305,7 @@ __device__ __forceinline__ void tile_far(const float4 *__restrict__ sa,
       a[r].gx = fmaf(ft, dx, a[r].gx);
       a[r].gy = fmaf(ft, dy, a[r].gy);
       a[r].gz = fmaf(ft, dz, a[r].gz);
-      if (DIFF) {
+      if (DIFF && !NZ) {
         a[r].ex = fmaf(dp, s.x, a[r].ex);
         a[r].ey = fmaf(dp, s.y, a[r].ey);
         a[r].ez = fmaf(dp, s.z, a[r].ez);
@@ -306,7 +346,7 @@ struct Target2 {
 
 __device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
 
-template <bool DIFF, bool UNI, bool RCP, int NSRC, int U, int KERN>
+template <bool DIFF, bool UNI, bool RCP, int NSRC, int U, int KERN, bool NZ>
 __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
                                                 const float4 *__restrict__ f1,
                                                 const float4 *__restrict__ f2,
@@ -329,7 +369,26 @@ __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
     const float2 dz = __fadd2_rn(T.z, npz);
     const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
     float2 qh, nfh, dp;
-    if (UNI) {
+    if (NZ) {
+      // Z-free far field in pairs (kernel_scalars_nz), no diffusion sums
+      if (UNI) {
+        const float2 sr = __fadd2_rn(r2, s2u);
+        const float2 y = make_float2(rcp_approx(sr.x), rcp_approx(sr.y));
+        const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+        const float2 ri2 = __fmul2_rn(ri, ri);
+        const float2 ph = __ffma2_rn(__fmul2_rn(h2, y), y, y);
+        qh = __fmul2_rn(__fmul2_rn(ph, ri), ri2);
+        nfh = __fmul2_rn(qh, ri2);
+      } else {
+        const float2 sig2 = __fadd2_rn(T.h, hj);
+        float qa, fa, qb, fb;
+        kernel_scalars_nz(sig2.x, r2.x, qa, fa);
+        kernel_scalars_nz(sig2.y, r2.y, qb, fb);
+        qh = make_float2(qa, qb);
+        nfh = make_float2(fa, fb);
+      }
+      dp = make_float2(0.f, 0.f);
+    } else if (UNI) {
       // kernel_scalars_uniform in pairs, returning -fs
       const float2 sr = __fadd2_rn(r2, s2u);
       const float2 w = make_float2(rsqrtf(sr.x), rsqrtf(sr.y));
@@ -384,7 +443,7 @@ __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
     a.gx = __ffma2_rn(nft, dx, a.gx);
     a.gy = __ffma2_rn(nft, dy, a.gy);
     a.gz = __ffma2_rn(nft, dz, a.gz);
-    if (DIFF) {
+    if (DIFF && !NZ) {
       a.ex = __ffma2_rn(dp, sx, a.ex);
       a.ey = __ffma2_rn(dp, sy, a.ey);
       a.ez = __ffma2_rn(dp, sz, a.ez);
@@ -495,11 +554,9 @@ __device__ __forceinline__ float box_gap2(float4 alo, float4 ahi, float4 blo, fl
 
 // Far formulation allowed: box gap positive and at least max(near radius,
 // half-diagonal of the source box).
-__device__ __forceinline__ bool far_tiles(float4 tlo, float4 thi, float4 slo, float4 shi,
-                                          float near2) {
+__device__ __forceinline__ bool far_tiles(float gap2, float4 slo, float4 shi, float near2) {
   const float ex = shi.x - slo.x, ey = shi.y - slo.y, ez = shi.z - slo.z;
   const float half_diag2 = 0.25f * (ex * ex + ey * ey + ez * ez);
-  const float gap2 = box_gap2(tlo, thi, slo, shi);
   return gap2 > 0.f && gap2 >= near2 && gap2 >= half_diag2;
 }
 
@@ -591,7 +648,11 @@ __global__ void __launch_bounds__(TB, MINB)
       const float4 slo = __ldg(sg.boxes + 2 * (ts / TB));
       const float4 shi = __ldg(sg.boxes + 2 * (ts / TB) + 1);
       const bool diag = (ts < w.t0 + TPB) && (w.t0 < ts + TB);
-      const bool near = diag || !far_tiles(tlo, thi, slo, shi, sg.near2);
+      const float gap2 = box_gap2(tlo, thi, slo, shi);
+      const bool near = diag || !far_tiles(gap2, slo, shi, sg.near2);
+      // every pair at rho >= 6 sigma: the Z-free far field (w of a box = the
+      // range of h = s^2/2, so thi.w + shi.w is the largest sigma^2)
+      const bool nz = KERN == KERNEL_HIGHORDER && !near && gap2 >= 36.f * (thi.w + shi.w);
       // one smoothing radius over both tiles
       const bool uni = KERN == KERNEL_HIGHORDER && tlo.w == thi.w && slo.w == shi.w && tlo.w == slo.w;
       const float cx = 0.5f * (slo.x + shi.x), cy = 0.5f * (slo.y + shi.y),
@@ -659,14 +720,17 @@ __global__ void __launch_bounds__(TB, MINB)
         Acc2 b;
         b.wx = b.wy = b.wz = b.qx = b.qy = b.qz = b.gx = b.gy = b.gz = make_float2(0.f, 0.f);
         b.ex = b.ey = b.ez = b.ev = make_float2(0.f, 0.f);
-        if (uni)
-          tile_far_packed<DIFF, true, PK == 1, TB, U, KERN>(fq + buf * FQ, fq + (2 + buf) * FQ,
-                                                      fq + (4 + buf) * FQ, fq + (6 + buf) * FQ,
-                                                      fq + (8 + buf) * FQ, fz + buf * FQ, T2, slo.w, b);
+        const float4 *f0 = fq + buf * FQ, *f1 = fq + (2 + buf) * FQ, *f2 = fq + (4 + buf) * FQ,
+                     *f3 = fq + (6 + buf) * FQ, *f4 = fq + (8 + buf) * FQ;
+        const float2 *f5 = fz + buf * FQ;
+        if (nz && uni)
+          tile_far_packed<DIFF, true, PK == 1, TB, U, KERN, true>(f0, f1, f2, f3, f4, f5, T2, slo.w, b);
+        else if (nz)
+          tile_far_packed<DIFF, false, PK == 1, TB, U, KERN, true>(f0, f1, f2, f3, f4, f5, T2, 0.f, b);
+        else if (uni)
+          tile_far_packed<DIFF, true, PK == 1, TB, U, KERN, false>(f0, f1, f2, f3, f4, f5, T2, slo.w, b);
         else
-          tile_far_packed<DIFF, false, PK == 1, TB, U, KERN>(fq + buf * FQ, fq + (2 + buf) * FQ,
-                                                       fq + (4 + buf) * FQ, fq + (6 + buf) * FQ,
-                                                       fq + (8 + buf) * FQ, fz + buf * FQ, T2, 0.f, b);
+          tile_far_packed<DIFF, false, PK == 1, TB, U, KERN, false>(f0, f1, f2, f3, f4, f5, T2, 0.f, b);
         const double s2 = uni ? 2.0 * (double)slo.w : 1.0;
         const double As2 = A * s2;
         const double cd = uni ? 32.0 * cnu : cnu;
@@ -679,7 +743,7 @@ __global__ void __launch_bounds__(TB, MINB)
         oa[0][0] += (ay[0] * Qz - az[0] * Qy) - 3.0 * As2 * (b.gx.x + b.gx.y);
         oa[0][1] += (az[0] * Qx - ax[0] * Qz) - 3.0 * As2 * (b.gy.x + b.gy.y);
         oa[0][2] += (ax[0] * Qy - ay[0] * Qx) - 3.0 * As2 * (b.gz.x + b.gz.y);
-        if (DIFF) {
+        if (DIFF && !nz) {
           const double v = T[0].v, ev = b.ev.x + b.ev.y;
           oa[0][0] += cd * (v * (b.ex.x + b.ex.y) - ev * ax[0]);
           oa[0][1] += cd * (v * (b.ey.x + b.ey.y) - ev * ay[0]);
@@ -696,12 +760,15 @@ __global__ void __launch_bounds__(TB, MINB)
           F[r].gy = fmaf(F[r].z, T[r].ah, -F[r].x * T[r].ch);
           F[r].gz = fmaf(F[r].x, T[r].bh, -F[r].y * T[r].ah);
         }
-        if (uni)
-          tile_far<DIFF, true, P, R, TB, U, KERN>(sp + buf * TB, sv + buf * TB, spl + buf * TB, g, T, F,
-                                            slo.w, a);
+        const float4 *ta = sp + buf * TB, *tb = sv + buf * TB, *tc = spl + buf * TB;
+        if (nz && uni)
+          tile_far<DIFF, true, P, R, TB, U, KERN, true>(ta, tb, tc, g, T, F, slo.w, a);
+        else if (nz)
+          tile_far<DIFF, false, P, R, TB, U, KERN, true>(ta, tb, tc, g, T, F, 0.f, a);
+        else if (uni)
+          tile_far<DIFF, true, P, R, TB, U, KERN, false>(ta, tb, tc, g, T, F, slo.w, a);
         else
-          tile_far<DIFF, false, P, R, TB, U, KERN>(sp + buf * TB, sv + buf * TB, spl + buf * TB, g, T, F,
-                                             0.f, a);
+          tile_far<DIFF, false, P, R, TB, U, KERN, false>(ta, tb, tc, g, T, F, 0.f, a);
         // undo the uniform-radius scaling: qh = sigma^2 qs, fh = sigma^2 fs, Dp = 32 ds
         const double s2 = uni ? 2.0 * (double)slo.w : 1.0;
         const double As2 = A * s2;
@@ -717,7 +784,7 @@ __global__ void __launch_bounds__(TB, MINB)
           oa[r][0] += (ay[r] * Qz - az[r] * Qy) + 3.0 * As2 * a[r].gx;
           oa[r][1] += (az[r] * Qx - ax[r] * Qz) + 3.0 * As2 * a[r].gy;
           oa[r][2] += (ax[r] * Qy - ay[r] * Qx) + 3.0 * As2 * a[r].gz;
-          if (DIFF) {
+          if (DIFF && !nz) {
             const double v = T[r].v;
             oa[r][0] += cd * (v * a[r].ex - (double)a[r].ev * ax[r]);
             oa[r][1] += cd * (v * a[r].ey - (double)a[r].ev * ay[r]);
@@ -807,6 +874,10 @@ KernelFn select_highorder(const PairConfig &c) {
   PAWAN_F32_CASE_PK(256, 1, 1, 4, 2, 1)
   PAWAN_F32_CASE_PK(256, 1, 1, 2, 2, 2)
   PAWAN_F32_CASE_PK(256, 1, 1, 4, 2, 2)
+  PAWAN_F32_CASE_PK(128, 1, 1, 8, 4, 2)
+  PAWAN_F32_CASE_PK(128, 1, 1, 4, 3, 2)
+  PAWAN_F32_CASE_PK(128, 1, 1, 8, 3, 2)
+  PAWAN_F32_CASE_PK(256, 1, 1, 8, 2, 2)
   PAWAN_F32_CASE(128, 1, 1, 2, 4)
   PAWAN_F32_CASE(128, 1, 1, 4, 4)
   PAWAN_F32_CASE(128, 2, 1, 2, 4)
@@ -828,13 +899,14 @@ KernelFn select_highorder(const PairConfig &c) {
   return nullptr;
 }
 
-// The Gaussian kernel is compiled for the default tilings only.
+// The Gaussian kernel is compiled for the default tilings only (packed mode 2:
+// its far tiles never take the uniform-radius branch that modes 1 and 2 differ in).
 template <bool DIFF>
 KernelFn select_gaussian(const PairConfig &c) {
-  PAWAN_F32_CASE_K(128, 1, 1, 4, 4, 1, KERNEL_GAUSSIAN)
+  PAWAN_F32_CASE_K(128, 1, 1, 4, 4, 2, KERNEL_GAUSSIAN)
   PAWAN_F32_CASE_K(128, 1, 1, 2, 4, 0, KERNEL_GAUSSIAN)
   PAWAN_F32_CASE_K(128, 2, 1, 4, 4, 0, KERNEL_GAUSSIAN)
-  PAWAN_F32_CASE_K(256, 1, 1, 4, 2, 1, KERNEL_GAUSSIAN)
+  PAWAN_F32_CASE_K(256, 1, 1, 4, 2, 2, KERNEL_GAUSSIAN)
   return nullptr;
 }
 #undef PAWAN_F32_CASE

@@ -42,7 +42,7 @@ int cuda_fail(pawan_ctx *ctx, cudaError_t e, const char *where) {
 TileChoice default_tile(int precision) {
   TileChoice t;
   if (precision == PAWAN_PREC_F32) {
-    t.pc = PairConfig{128, 1, 4, 1, 0, 1};  // packed far path, unroll 4
+    t.pc = PairConfig{128, 1, 4, 1, 0, 2};  // packed far path, unroll 4
   } else {
     t.pc = PairConfig{128, 1, 1};
   }
@@ -457,7 +457,7 @@ int autotune_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, in
     }
   }
   if (status == PAWAN_OK) {
-    for (int ips : {4, 8, 32}) {
+    for (int ips : {4, 8, 32, 64}) {
       TileChoice t = best_t;
       t.items_per_slot = ips;
       double ms = 0;

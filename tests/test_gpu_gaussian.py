@@ -56,8 +56,8 @@ def test_gaussian_mixed_radii_near_and_far(ctx, prec):
     check(prec, *s.union_rates(), *oracle.pairs(pos, vor, rad, vol, sc.nu, kernel="gaussian"))
 
 
-@pytest.mark.parametrize("tiling", [(128, 1, 1, 4, 0, 1), (128, 1, 1, 2, 0, 0), (128, 2, 1, 4, 0, 0),
-                                    (256, 1, 1, 4, 0, 1)])
+@pytest.mark.parametrize("tiling", [(128, 1, 1, 4, 0, 2), (128, 1, 1, 2, 0, 0), (128, 2, 1, 4, 0, 0),
+                                    (256, 1, 1, 4, 0, 2)])
 def test_gaussian_every_compiled_tiling(ctx, tiling):
     sc = g.ring_pair(n_stations=70, seed=82, nu=1e-3)  # N = 1,120
     pos, vor, rad, vol = sc.union()

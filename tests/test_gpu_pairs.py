@@ -11,6 +11,7 @@ import pytest
 import oracle
 import pawan_b200
 from pawan_b200 import System
+from pawan_b200 import union_to_state as union_state
 from pawan_b200 import geometry as g
 from helpers import load, max_rel, rms_rel, split_rates, tol
 
@@ -236,3 +237,51 @@ def test_full_size_sampled_targets(ctx, name):
     check("f32", u[t], da[t], u_ref, da_ref)
     _, da_all = u, da
     assert np.abs(da_all.sum(axis=0)).max() < 1e-5 * np.abs(da_all).sum()
+
+
+@pytest.mark.parametrize("gap", [3.0, 4.5, 5.5, 6.5, 10.0])
+def test_tile_classes_at_their_boundaries(ctx, gap):
+    """Two compact clusters of 256 particles (two 128-tiles each) whose boxes
+    are `gap` smoothing radii apart: near (< 4 s), far with the Z terms
+    (4 s .. 6 s) and far without them (>= 6 s, where Z is below 3e-9 of q).
+    The whole solve against the FP64 oracle; then the cross-cluster part at
+    cluster A on its own, by linearity: the same system solved with cluster
+    B's strengths doubled, minus the first solve, is at A exactly the part of
+    A's rates that B's strengths drive (A's own tiles compute identically in
+    both solves), compared with the same difference in the oracle.  nu != 0;
+    packed and scalar tilings."""
+    rng = np.random.default_rng(int(gap * 10))
+    s = 0.05
+    n = 256
+    a = rng.uniform(-0.5 * s, 0.5 * s, (n, 3))
+    b = rng.uniform(-0.5 * s, 0.5 * s, (n, 3))
+    b[:, 0] += (gap + 1.0) * s  # box gap = gap * s
+    pos = np.concatenate([a, b])
+    vor = rng.normal(size=(2 * n, 3)) * 1e-3
+    vor2 = vor.copy()
+    vor2[n:] *= 2.0
+    rad = np.full(2 * n, s)
+    vol = np.full(2 * n, 1e-5)
+    nu = 1e-3
+    u1, da1 = oracle.pairs(pos, vor, rad, vol, nu)
+    u2, da2 = oracle.pairs(pos, vor2, rad, vol, nu)
+    du_ref, dda_ref = (u2 - u1)[:n], (da2 - da1)[:n]
+    st1, st2 = union_state([2 * n], pos, vor), union_state([2 * n], pos, vor2)
+    sysm = System(ctx, [2 * n], nu, "f32")
+    sysm.set_particles(pos, vor, rad, vol)
+    configs = [dict(threads=tb, threads_per_target=1, unroll=unroll, items_per_slot=16,
+                    blocks_per_sm=minb, packed=mode) for tb, unroll, minb, mode in F32_PACKED[:4]]
+    configs += [dict(threads=tb, threads_per_target=p, unroll=unroll, items_per_slot=16,
+                     targets_per_thread=r, blocks_per_sm=minb) for tb, p, r, unroll, minb in F32_TILINGS[:6]]
+    for cfg in configs:
+        sysm.set_config(**cfg)
+        sysm.set_states(st1)
+        sysm.solve()
+        ug1, dag1 = sysm.union_rates()
+        check("f32", ug1, dag1, u1, da1)
+        sysm.set_states(st2)
+        sysm.solve()
+        ug2, dag2 = sysm.union_rates()
+        du, dda = (ug2 - ug1)[:n], (dag2 - dag1)[:n]
+        assert rms_rel(du, du_ref) < 1e-5 and rms_rel(dda, dda_ref) < 1e-5, \
+            (cfg, rms_rel(du, du_ref), rms_rel(dda, dda_ref))
