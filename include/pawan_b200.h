@@ -271,6 +271,17 @@ int pawan_server_fetch(pawan_server *srv, long long id, double *state, size_t si
                        double *t_submit, double *t_admit, double *t_done);
 int pawan_server_cancel(pawan_server *srv, long long id);
 int pawan_server_stats(pawan_server *srv, pawan_serve_stats *out);
+/* Host-side fault injection, for testing how callers and the engine recover
+ * (no GPU fault is made).  PAWAN_FAULT_ALLOC: the next `count` admissions
+ * fail as an out-of-memory from the device allocator would (the request is
+ * rejected, the others go on).  PAWAN_FAULT_ITERATION: the next `count`
+ * iterations fail as a failed launch would (every request active in it is
+ * rejected; the engine carries on with the next).  PAWAN_FAULT_SLOW: the next
+ * `count` iterations first sleep `seconds` on the host (at most 60). */
+#define PAWAN_FAULT_ALLOC 1
+#define PAWAN_FAULT_ITERATION 2
+#define PAWAN_FAULT_SLOW 3
+int pawan_server_inject(pawan_server *srv, int fault, int count, double seconds);
 
 /* ------------------------------------------------- allocation-free solve */
 /* No counterpart in the reference.  For callers that must not allocate device

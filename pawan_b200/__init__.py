@@ -114,6 +114,7 @@ _SIGS = {
     "pawan_system_influence": (ctypes.c_int, [_vp, _dp, ctypes.c_size_t]),
     "pawan_shard_size": (ctypes.c_size_t, [ctypes.c_size_t, ctypes.c_int]),
     "pawan_system_set_kernel": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pawan_server_inject": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
     "pawan_system_get_kernel": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     "pawan_system_set_shard": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
     "pawan_system_shard_rates": (ctypes.c_int, [_vp]),
@@ -556,6 +557,16 @@ class Server:
         st = self._lib.pawan_server_cancel(self._h, rid)
         if st != OK:
             raise PawanError(st, f"request {rid}")
+
+    FAULTS = {"alloc": 1, "iteration": 2, "slow": 3}
+
+    def inject(self, fault: str, count: int = 1, seconds: float = 0.0):
+        """Host-side fault injection: "alloc" (admission allocation fails),
+        "iteration" (an engine iteration fails), "slow" (iterations sleep
+        `seconds` first)."""
+        st = self._lib.pawan_server_inject(self._h, self.FAULTS[fault], int(count), float(seconds))
+        if st != OK:
+            raise PawanError(st, "inject")
 
     def stats(self) -> dict:
         s = ServeStats()

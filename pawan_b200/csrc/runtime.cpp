@@ -3,6 +3,8 @@
 // systems, RK4 driving, diagnostics, autotuning and throughput probes.
 #include "runtime.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -377,9 +379,20 @@ int launch_stage_mode(pawan_ctx *ctx, Plan &p, int mode) {
   return PAWAN_OK;
 }
 
+// NVTX range over a scope (header-only NVTX; a no-op unless a profiler is
+// attached): one per RK4 step and one per stage, so a timeline shows the
+// reference's stage structure (rk4.cpp:24-66).
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+
 static int rk4_one_step(pawan_ctx *ctx, Plan &p, bool allow_events) {
   static const int modes[4] = {STAGE_K1, STAGE_K2, STAGE_K3, STAGE_FINAL};
+  static const char *names[4] = {"pawan rk4 k1", "pawan rk4 k2", "pawan rk4 k3", "pawan rk4 k4+update"};
+  NvtxRange step("pawan rk4 step");
   for (int s = 0; s < 4; ++s) {
+    NvtxRange stage(names[s]);
     PAWAN_TRY(launch_pairs(ctx, p, allow_events));
     PAWAN_TRY(launch_stage_mode(ctx, p, modes[s]));
   }

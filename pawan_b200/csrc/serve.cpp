@@ -99,9 +99,19 @@ struct pawan_server {
   TileChoice tile;
   double rate = kRateGuess;  // measured interactions/s of the iterations (worker only)
   cudaMemPool_t pool = nullptr;
+  // host-side fault injection (pawan_server_inject), under `mu`
+  int fail_alloc = 0, fail_iteration = 0, slow_iterations = 0;
+  double slow_seconds = 0.0;
 };
 
 namespace {
+
+// Consumes one pending injected fault of a kind (call with `mu` held).
+bool take(int &pending) {
+  if (pending <= 0) return false;
+  --pending;
+  return true;
+}
 
 void finish(pawan_server *srv, Request *r, int state) {
   r->state = state;
@@ -188,8 +198,14 @@ void worker_main(pawan_server *srv) {
     // create device state of newly admitted requests (outside the lock)
     const auto ta0 = std::chrono::steady_clock::now();
     for (Request *r : admit) {
-      int st = system_create_ordered(srv->ctx, r->counts.size(), r->counts.data(), r->nu,
-                                     srv->cfg.precision, &r->sys);
+      bool injected;
+      {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        injected = take(srv->fail_alloc);
+      }
+      int st = injected ? fail(srv->ctx, PAWAN_ERR_NOMEM, "injected allocation failure")
+                        : system_create_ordered(srv->ctx, r->counts.size(), r->counts.data(),
+                                                r->nu, srv->cfg.precision, &r->sys);
       if (st == PAWAN_OK)
         st = system_upload(r->sys, r->pos.data(), r->vor.data(), r->rad.data(), r->vol.data());
       std::lock_guard<std::mutex> lk(srv->mu);
@@ -228,6 +244,16 @@ void worker_main(pawan_server *srv) {
     size_t k = 0;
     double n2 = 0.0;
     for (Request *r : act) n2 += (double)r->n * (double)r->n;
+    bool inj_fail = false, inj_slow = false;
+    double slow_s = 0.0;
+    {
+      std::lock_guard<std::mutex> lk(srv->mu);
+      inj_fail = take(srv->fail_iteration);
+      inj_slow = take(srv->slow_iterations);
+      slow_s = srv->slow_seconds;
+    }
+    if (inj_slow) std::this_thread::sleep_for(std::chrono::duration<double>(slow_s));
+    if (st == PAWAN_OK && inj_fail) st = fail(srv->ctx, PAWAN_ERR_CUDA, "injected iteration failure");
     if (st == PAWAN_OK) {
       k = steps_per_iteration(srv, act);
       st = run_iteration(srv, *plan, k);
@@ -461,6 +487,28 @@ int pawan_server_cancel(pawan_server *srv, long long id) {
   } else if (r->state == PAWAN_REQ_ACTIVE) {
     r->cancel = true;
   }
+  return PAWAN_OK;
+}
+
+int pawan_server_inject(pawan_server *srv, int fault, int count, double seconds) {
+  if (!srv || count < 0) return PAWAN_ERR_INVALID;
+  std::lock_guard<std::mutex> lk(srv->mu);
+  switch (fault) {
+    case PAWAN_FAULT_ALLOC:
+      srv->fail_alloc = count;
+      break;
+    case PAWAN_FAULT_ITERATION:
+      srv->fail_iteration = count;
+      break;
+    case PAWAN_FAULT_SLOW:
+      if (!(seconds >= 0.0) || seconds > 60.0) return PAWAN_ERR_INVALID;
+      srv->slow_iterations = count;
+      srv->slow_seconds = seconds;
+      break;
+    default:
+      return PAWAN_ERR_INVALID;
+  }
+  srv->cv_work.notify_all();
   return PAWAN_OK;
 }
 

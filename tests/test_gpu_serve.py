@@ -140,3 +140,52 @@ def test_queue_limit_and_cancel(ctx):
         if st == 0:
             assert srv.wait(rid, 60)
     srv.close()
+
+
+def test_injected_allocation_failure_rejects_one_request(ctx):
+    """A failed device allocation at admission (made on the host) rejects that
+    request only; the others complete with the same results as alone."""
+    scs = requests(k=3, seed=11)
+    srv = Server(ctx, budget_bytes=1 << 30)
+    srv.inject("alloc", 1)
+    ids = [srv.submit_scenario(sc)[1] for sc in scs]
+    for rid in ids:
+        assert srv.wait(rid, 60)
+    states = [srv.poll(rid) for rid in ids]
+    assert states.count("rejected") == 1 and states.count("done") == 2
+    outs = [srv.fetch(rid)[0] for rid in ids]
+    srv.close()
+    for sc, out, st in zip(scs, outs, states):
+        if st == "done":
+            assert np.array_equal(out, run_alone(ctx, sc))
+        else:
+            assert out is None
+
+
+def test_injected_iteration_failure_then_recovery(ctx):
+    """A failed iteration rejects the requests active in it; the engine then
+    serves new requests normally."""
+    sc = g.single_ring(n_stations=64, seed=12, steps=5)
+    srv = Server(ctx, budget_bytes=1 << 30, iteration_seconds=1e-9)
+    srv.inject("iteration", 1)
+    rid = srv.submit_scenario(sc)[1]
+    assert srv.wait(rid, 60)
+    assert srv.poll(rid) == "rejected"
+    rid2 = srv.submit_scenario(sc)[1]
+    assert srv.wait(rid2, 60)
+    assert srv.poll(rid2) == "done"
+    out, *_ = srv.fetch(rid2)
+    srv.close()
+    assert np.array_equal(out, run_alone(ctx, sc))
+
+
+def test_injected_slow_iteration_times_out_the_wait(ctx):
+    """A slow iteration: a short wait times out, a longer one completes."""
+    sc = g.single_ring(n_stations=32, seed=13, steps=2)
+    srv = Server(ctx, budget_bytes=1 << 30)
+    srv.inject("slow", 1, seconds=1.0)
+    rid = srv.submit_scenario(sc)[1]
+    assert srv.wait(rid, 0.2) is False
+    assert srv.wait(rid, 30)
+    assert srv.poll(rid) == "done"
+    srv.close()
