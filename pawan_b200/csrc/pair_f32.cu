@@ -375,7 +375,7 @@ __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
         const float2 sr = __fadd2_rn(r2, s2u);
         const float2 y = make_float2(rcp_approx(sr.x), rcp_approx(sr.y));
         const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-        const float2 ri2 = __fmul2_rn(ri, ri);
+        const float2 ri2 = RCP ? make_float2(rcp_approx(r2.x), rcp_approx(r2.y)) : __fmul2_rn(ri, ri);
         const float2 ph = __ffma2_rn(__fmul2_rn(h2, y), y, y);
         qh = __fmul2_rn(__fmul2_rn(ph, ri), ri2);
         nfh = __fmul2_rn(qh, ri2);
