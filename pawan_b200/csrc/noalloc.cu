@@ -25,6 +25,7 @@
 // The arithmetic is that of pawan_system_solve in PAWAN_PREC_F32 (same pair
 // kernel), with a fixed tiling (128 threads, one target per thread) and
 // 4,096-source chunks.
+#include <cstddef>
 #include <mutex>
 
 #include "../../include/pawan_b200.h"
@@ -42,7 +43,9 @@ constexpr int kNaMaxChunks = (kNoallocMaxParticles + kNaChunk - 1) / kNaChunk;
 constexpr int kNaMaxItems = kNaMaxTiles * kNaMaxChunks;
 constexpr int kNaPrepBlocks = (kNoallocMaxParticles + kStageThreads - 1) / kStageThreads;
 
-// Layout of the scratch array (every part 256-byte aligned).
+// Layout of the scratch array.  The kernels need 16-byte alignment of the
+// float4 arrays (their offsets are multiples of 256 bytes) and natural
+// alignment of the rest.
 struct NoallocScratch {
   float4 pos32[kNoallocMaxParticles];
   float4 vor32[kNoallocMaxParticles];
@@ -55,6 +58,9 @@ struct NoallocScratch {
   SegDesc seg;
   int counter;
 };
+
+static_assert(offsetof(NoallocScratch, boxes) % 256 == 0 && offsetof(NoallocScratch, partial) % 256 == 0,
+              "scratch arrays on 256-byte boundaries");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoallocScratch)];
 

@@ -3,7 +3,7 @@
 Runs the reference's own C++ classes (compiled from their unmodified sources
 into oracle/_ref/libpawan_ref.so by `make -C oracle`) on small seeded inputs
 and stores inputs and outputs.  The fixtures pin the oracle restatement and the
-GPU path on machines without the reference tree (the GPU box).
+GPU path on machines without the reference tree.
 
     python tests/golden/gen_golden.py [case ...]     (no case: all of them)
 
