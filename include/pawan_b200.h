@@ -159,6 +159,19 @@ int pawan_system_set_precision(pawan_system *sys, int precision);
  * radius (N f64): __integration::integrate's per-step output
  * (integration.cpp:20-21, 28-29; interaction.cpp:197-202; wake.cpp:68-73). */
 int pawan_system_write_frame(pawan_system *sys, const char *path, double t, int append);
+/* __integration::integrate (src/integration/integration.cpp:16-35): n steps of
+ * dt = T/n -- RK4 as __rk4::step (PAWAN_INTEGRATE_RK4) or Euler as
+ * __integration::step (PAWAN_INTEGRATE_EULER) -- with a .wake frame at t = 0 and
+ * after every step at t = i*dt, in the reference's frame format, written to
+ * `path` (created or truncated).  The steps stay on the device; each frame is
+ * copied out through a pinned ring and written by a background thread while
+ * the next steps run.  The _file variant writes to an open FILE* (a
+ * `FILE *` of the caller's C library, e.g. from __io::create_binary_file, which
+ * stays open). */
+#define PAWAN_INTEGRATE_RK4 0
+#define PAWAN_INTEGRATE_EULER 1
+int pawan_system_integrate(pawan_system *sys, double T, size_t n, const char *path, int method);
+int pawan_system_integrate_file(pawan_system *sys, double T, size_t n, void *file, int method);
 int pawan_system_set_tiling(pawan_system *sys, const pawan_tiling *tiling);
 int pawan_system_get_tiling(pawan_system *sys, pawan_tiling *tiling);
 /* Times every compiled tiling on this system and keeps the fastest. */

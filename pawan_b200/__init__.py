@@ -114,6 +114,9 @@ _SIGS = {
     "pawan_system_influence": (ctypes.c_int, [_vp, _dp, ctypes.c_size_t]),
     "pawan_shard_size": (ctypes.c_size_t, [ctypes.c_size_t, ctypes.c_int]),
     "pawan_system_set_kernel": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pawan_system_integrate": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_size_t, ctypes.c_char_p,
+                                              ctypes.c_int]),
+    "pawan_system_integrate_file": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_size_t, _vp, ctypes.c_int]),
     "pawan_server_inject": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
     "pawan_system_get_kernel": (ctypes.c_int, [_vp, ctypes.POINTER(ctypes.c_int)]),
     "pawan_system_set_shard": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp]),
@@ -379,6 +382,12 @@ class System:
         v = ctypes.c_double()
         self.ctx.check(self._lib.pawan_system_kinetic_energy(self._h, ctypes.byref(v)))
         return v.value
+
+    def integrate(self, T: float, n: int, path: str, method: str = "rk4"):
+        """The reference's integrate(): n steps of T/n with a .wake frame at t = 0
+        and after every step, written to `path` asynchronously."""
+        m = {"rk4": 0, "euler": 1}[method]
+        self.ctx.check(self._lib.pawan_system_integrate(self._h, float(T), int(n), os.fsencode(path), m))
 
     def set_kernel(self, kernel: str):
         """Smoothing kernel: "highorder" (the reference's default) or "gaussian"."""

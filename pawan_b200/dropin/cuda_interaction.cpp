@@ -169,6 +169,21 @@ double __cuda::kineticEnergy() {
   return ke;
 }
 
+void __cuda_rk4::integrate(__system *S, __io *IO) {
+  __cuda *C = dynamic_cast<__cuda *>(S);
+  if (!C) {
+    __rk4::integrate(S, IO);
+    return;
+  }
+  C->upload();
+  FILE *f = IO->create_binary_file(".wake");
+  if (!f) throw std::runtime_error("pawan_b200: cannot create the .wake file (does its directory exist?)");
+  const int st = pawan_system_integrate_file(C->device_system(), _t, _n, f, PAWAN_INTEGRATE_RK4);
+  std::fclose(f);
+  if (st != PAWAN_OK) throw std::runtime_error("pawan_b200: integrate failed");
+  C->download();
+}
+
 void __cuda_rk4::step(const double &dt, __system *S, gsl_vector *state) {
   __cuda *C = dynamic_cast<__cuda *>(S);
   if (!C) {

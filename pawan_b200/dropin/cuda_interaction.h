@@ -82,6 +82,13 @@ class __cuda_rk4 : public __rk4 {
  public:
   __cuda_rk4(const double &t, const size_t &n) : __rk4(t, n) {}
   ~__cuda_rk4() = default;
+  /* __integration::integrate (integration.cpp:16-35) for a __cuda system: the
+   * n steps stay on the device and the .wake frames (same file, same bytes
+   * layout) are written by a background thread while the next steps run; the
+   * wakes hold the final state afterwards.  Any other system goes through the
+   * reference's integrate().  integrate() is not virtual in the reference, so
+   * call it through a __cuda_rk4 (not an __integration) pointer or reference. */
+  void integrate(__system *S, __io *IO);
 
  protected:
   void step(const double &dt, __system *S, gsl_vector *state) override;

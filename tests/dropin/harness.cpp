@@ -185,6 +185,31 @@ int dropin_diagnose(int nw, const size_t *counts, const double *pos, const doubl
   }
 }
 
+// __cuda_rk4(T, n).integrate(__cuda) through the reference's non-virtual
+// integrate() (an __integration pointer: host loop, frames from the wakes; mode
+// 0) or through __cuda_rk4::integrate (device loop, asynchronous frames; mode
+// 1) -- writes data/temp.wake under the cwd.
+int dropin_integrate2(int nw, const size_t *counts, const double *pos, const double *vor,
+                      const double *rad, const double *vol, double nu, int precision, double T,
+                      size_t n, int mode) {
+  try {
+    auto W = make_wakes(nw, counts, pos, vor, rad, vol);
+    ReadCuda *G = make_cuda(W, nu, precision);
+    pawan::__io io;
+    pawan::__cuda_rk4 rk(T, n);
+    if (mode == 1)
+      rk.integrate(G, &io);
+    else
+      static_cast<pawan::__integration &>(rk).integrate(G, &io);
+    delete G;
+    for (auto *w : W) delete w;
+    return 0;
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return 1;
+  }
+}
+
 // __cuda_rk4(T, n).integrate(__cuda) -- writes data/temp.wake under the cwd.
 int dropin_integrate(int nw, const size_t *counts, const double *pos, const double *vor,
                      const double *rad, const double *vol, double nu, int precision, double T,

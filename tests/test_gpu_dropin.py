@@ -101,3 +101,37 @@ def test_integrate_writes_reference_wake_file(lib):
     ref = d["wake_bytes"].tobytes()
     assert len(raw) == len(ref)
     assert np.allclose(np.frombuffer(raw, np.float64), np.frombuffer(ref, np.float64), rtol=1e-12, atol=1e-15)
+
+
+@needs_lib
+@pytest.mark.parametrize("mode", [0, 1])
+def test_integrate_host_and_device_loops_write_the_reference_file(lib, mode):
+    """__cuda_rk4 through an __integration reference (the reference's own
+    integrate() loop, frames from the wakes) and through __cuda_rk4::integrate
+    (device loop, frames written asynchronously): both files match the one the
+    reference's integrate() wrote (layout exactly, values to FP64 rounding)."""
+    lib.dropin_integrate2.argtypes = [ctypes.c_int, _szp, _dp, _dp, _dp, _dp, ctypes.c_double, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_size_t, ctypes.c_int]
+    d = load("ring16_integrate")
+    cnt = np.asarray([int(c) for c in d["counts"]], dtype=np.uintp)
+    arrs = [np.ascontiguousarray(d[k]) for k in ("pos", "vor", "rad", "vol")]
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.makedirs(os.path.join(tmp, "data"))
+        os.chdir(tmp)
+        try:
+            rc = lib.dropin_integrate2(len(cnt), cnt.ctypes.data_as(_szp), *[x.ctypes.data_as(_dp) for x in arrs],
+                                       0.0, 2, float(d["T"]), int(d["nsteps"]), mode)
+        finally:
+            os.chdir(cwd)
+        assert rc == 0
+        raw = open(os.path.join(tmp, "data", "temp.wake"), "rb").read()
+    ref = d["wake_bytes"].tobytes()
+    assert len(raw) == len(ref)
+    a, b = np.frombuffer(raw, np.uint64), np.frombuffer(ref, np.uint64)
+    n = int(d["counts"].sum())
+    frame = 3 + 7 * n
+    for k in range(int(d["nsteps"]) + 1):  # nWake and N words are integers: exact
+        assert a[k * frame + 1] == b[k * frame + 1] and a[k * frame + 2] == b[k * frame + 2]
+    assert np.allclose(np.frombuffer(raw, np.float64)[0::frame], np.frombuffer(ref, np.float64)[0::frame])
+    assert np.allclose(np.frombuffer(raw, np.float64), np.frombuffer(ref, np.float64), rtol=1e-12, atol=1e-15)
