@@ -313,7 +313,7 @@ def run_batch_leg(ctx, n_solves: int = 512, steps: int = 4, seed: int = 4) -> di
 
 def run_serving_leg(ctx, rate: float, duration: float, n_lo: int, n_hi: int, steps_lo: int,
                     steps_hi: int, budget: float, cap: float, max_active: int, max_queue: int,
-                    drain: float, seed: int = 5) -> dict:
+                    drain: float, seed: int = 5, policy: str = "fifo") -> dict:
     """Replays a Poisson arrival trace against the continuous-batching server in
     real time.  Requests are built and submitted at their arrival times; when
     the server's queue is full an arrival is rejected without building it (the
@@ -324,7 +324,7 @@ def run_serving_leg(ctx, rate: float, duration: float, n_lo: int, n_hi: int, ste
     reqs = g.serving_requests(rate=rate, duration=duration, seed=seed, n_lo=n_lo, n_hi=n_hi,
                               steps_lo=steps_lo, steps_hi=steps_hi, build=False)
     srv = Server(ctx, budget_bytes=budget, max_step_interactions=cap, max_active=max_active,
-                 max_queue=max_queue)
+                 max_queue=max_queue, policy=policy)
     ids, rejected_full, rejected_engine = {}, 0, 0
     t0 = time.perf_counter()
     for r in reqs:
@@ -348,7 +348,9 @@ def run_serving_leg(ctx, rate: float, duration: float, n_lo: int, n_hi: int, ste
     deadline = time.perf_counter() + drain
     lat, done_inter = [], 0.0
     pending = dict(ids)
-    while pending and time.perf_counter() < deadline:
+    first = True  # requests that finished during the arrival window count too
+    while pending and (first or time.perf_counter() < deadline):
+        first = False
         for rid in list(pending):
             if srv.poll(rid) in ("done", "rejected", "cancelled"):
                 out, ts, ta, td = srv.fetch(rid)
@@ -362,7 +364,7 @@ def run_serving_leg(ctx, rate: float, duration: float, n_lo: int, n_hi: int, ste
     srv.close()
     lat.sort()
     pct = (lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None)
-    return {"rate_per_s": rate, "arrival_window_s": duration, "arrivals": len(reqs),
+    return {"policy": policy, "rate_per_s": rate, "arrival_window_s": duration, "arrivals": len(reqs),
             "N_range": [n_lo, n_hi], "steps_range": [steps_lo, steps_hi],
             "budget_bytes": budget, "max_step_interactions": cap, "max_active": max_active,
             "max_queue": max_queue, "submitted": len(ids), "completed": len(lat),
@@ -677,6 +679,9 @@ def run_configs(args):
     emit({"config": "serving_specified", **run_serving_leg(
         ctx, rate=200.0, duration=60.0, n_lo=1024, n_hi=262144, steps_lo=50, steps_hi=400,
         budget=120e9, cap=2e11, max_active=0, max_queue=64, drain=30.0)})
+    emit({"config": "serving_specified_shortest_first", **run_serving_leg(
+        ctx, rate=200.0, duration=60.0, n_lo=1024, n_hi=262144, steps_lo=50, steps_hi=400,
+        budget=120e9, cap=2e11, max_active=0, max_queue=64, drain=30.0, policy="shortest")})
     emit({"config": "serving_capacity_matched", **run_serving_leg(
         ctx, rate=120.0, duration=30.0, n_lo=1024, n_hi=16384, steps_lo=5, steps_hi=20,
         budget=120e9, cap=0.0, max_active=0, max_queue=0, drain=60.0)})

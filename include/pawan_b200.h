@@ -247,7 +247,13 @@ typedef struct {
   int precision;                /* PAWAN_PREC_* */
   double iteration_seconds;     /* device time one iteration may take before new arrivals
                                    are admitted (0: 20 ms; tiny: one step per iteration) */
+  int policy;                   /* admission order: PAWAN_SERVE_FIFO (arrival) or
+                                   PAWAN_SERVE_SHORTEST_FIRST (least N^2 x steps first; under
+                                   overload large requests can wait indefinitely) */
 } pawan_serve_config;
+
+#define PAWAN_SERVE_FIFO 0
+#define PAWAN_SERVE_SHORTEST_FIRST 1
 
 typedef struct {
   unsigned long long submitted, admitted, completed, rejected, queued, active;

@@ -51,7 +51,8 @@ class PawanError(RuntimeError):
 class ServeConfig(ctypes.Structure):
     _fields_ = [("budget_bytes", ctypes.c_double), ("max_step_interactions", ctypes.c_double),
                 ("max_active", ctypes.c_int), ("max_queue", ctypes.c_int),
-                ("precision", ctypes.c_int), ("iteration_seconds", ctypes.c_double)]
+                ("precision", ctypes.c_int), ("iteration_seconds", ctypes.c_double),
+                ("policy", ctypes.c_int)]
 
 
 class Tiling(ctypes.Structure):
@@ -493,14 +494,16 @@ class Server:
 
     def __init__(self, ctx: Context, budget_bytes: float, max_step_interactions: float = 0.0,
                  max_active: int = 0, max_queue: int = 0, precision: str = "f32",
-                 iteration_seconds: float = 0.0):
+                 iteration_seconds: float = 0.0, policy: str = "fifo"):
         """iteration_seconds: device time one engine iteration may take before
         new arrivals are admitted (0: the engine's default of 20 ms; a tiny value
-        gives one RK4 step per iteration)."""
+        gives one RK4 step per iteration).  policy: "fifo" (arrival order) or
+        "shortest" (least N^2 x steps first)."""
         self.ctx = ctx
         self._lib = ctx._lib
         cfg = ServeConfig(float(budget_bytes), float(max_step_interactions), int(max_active),
-                          int(max_queue), PREC[precision], float(iteration_seconds))
+                          int(max_queue), PREC[precision], float(iteration_seconds),
+                          {"fifo": 0, "shortest": 1}[policy])
         h = _vp()
         ctx.check(self._lib.pawan_server_create(ctx.handle, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h

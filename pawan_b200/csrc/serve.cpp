@@ -3,7 +3,8 @@
 //
 // Each request is a system (one ring, a ring pair, ...) with its own nu, dt
 // and step count.  The worker thread repeats: admit waiting requests in
-// arrival order while the device-memory budget, the active-request cap and the
+// arrival order (or least work first, N^2 x steps, with the shortest-first
+// policy) while the device-memory budget, the active-request cap and the
 // per-iteration work cap (sum N^2) allow; advance every admitted request by
 // k RK4 steps in one batched launch sequence per step (one persistent pair
 // launch per stage over all of them); retire the finished ones (state copied
@@ -169,8 +170,17 @@ void worker_main(pawan_server *srv) {
     std::vector<Request *> admit;
     {
       std::unique_lock<std::mutex> lk(srv->mu);
+      if (srv->cfg.policy == PAWAN_SERVE_SHORTEST_FIRST && srv->queue.size() > 1) {
+        // least work (N^2 x steps) first; arrival order among equals
+        std::stable_sort(srv->queue.begin(), srv->queue.end(), [&](long long a, long long b) {
+          const Request *ra = srv->reqs[a].get(), *rb = srv->reqs[b].get();
+          return (double)ra->n * (double)ra->n * (double)ra->nsteps <
+                 (double)rb->n * (double)rb->n * (double)rb->nsteps;
+        });
+      }
       for (;;) {
-        // admission in arrival order (no overtaking), within all caps
+        // admission in queue order (arrival order, or least work first), no
+        // overtaking of a request the caps hold back, within all caps
         if (srv->queue.empty()) break;
         Request *r = srv->reqs[srv->queue.front()].get();
         const size_t na = srv->active.size() + admit.size();
@@ -321,7 +331,8 @@ extern "C" {
 int pawan_server_create(pawan_ctx *ctx, const pawan_serve_config *cfg, pawan_server **out) {
   if (!ctx || !cfg || !out) return PAWAN_ERR_INVALID;
   if (!(cfg->budget_bytes > 0) || cfg->precision < PAWAN_PREC_F32 ||
-      cfg->precision > PAWAN_PREC_F64_PLAIN || !(cfg->iteration_seconds >= 0.0))
+      cfg->precision > PAWAN_PREC_F64_PLAIN || !(cfg->iteration_seconds >= 0.0) ||
+      (cfg->policy != PAWAN_SERVE_FIFO && cfg->policy != PAWAN_SERVE_SHORTEST_FIRST))
     return fail(ctx, PAWAN_ERR_INVALID, "bad serving configuration");
   std::unique_ptr<pawan_server> srv(new pawan_server());
   srv->cfg = *cfg;

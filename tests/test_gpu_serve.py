@@ -189,3 +189,30 @@ def test_injected_slow_iteration_times_out_the_wait(ctx):
     assert srv.wait(rid, 30)
     assert srv.poll(rid) == "done"
     srv.close()
+
+
+@pytest.mark.parametrize("policy", ["fifo", "shortest"])
+def test_admission_policy_orders_the_queue(ctx, policy):
+    """One request at a time: while the first runs, a large and then a small
+    request wait; FIFO admits the large one next, shortest-first the small one.
+    Results are the same under either policy."""
+    srv = Server(ctx, budget_bytes=1 << 30, max_active=1, iteration_seconds=1e-9, policy=policy)
+    first = g.single_ring(n_stations=64, seed=21, steps=300)
+    big = g.single_ring(n_stations=256, seed=22, steps=20)
+    small = g.single_ring(n_stations=32, seed=23, steps=5)
+    ra = srv.submit_scenario(first)[1]
+    deadline = time.time() + 30
+    while srv.poll(ra) == "queued" and time.time() < deadline:
+        time.sleep(0.0005)
+    rb = srv.submit_scenario(big)[1]
+    rc = srv.submit_scenario(small)[1]
+    for rid in (ra, rb, rc):
+        assert srv.wait(rid, 120)
+    outs = {rid: srv.fetch(rid) for rid in (ra, rb, rc)}
+    srv.close()
+    t_admit_big, t_admit_small = outs[rb][2], outs[rc][2]
+    if policy == "fifo":
+        assert t_admit_big < t_admit_small
+    else:
+        assert t_admit_small < t_admit_big
+    assert np.array_equal(outs[rc][0], run_alone(ctx, small))
