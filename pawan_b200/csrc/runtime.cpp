@@ -214,7 +214,11 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
   PAWAN_CUDA(ctx, p->partial.alloc(partial_total));
   PAWAN_CUDA(ctx, p->boxes.alloc(box_total));
   std::vector<WorkItem> wh(items.size());
-  for (size_t k = 0; k < items.size(); ++k) wh[k] = items[k].w;
+  p->item_costs.resize(items.size());
+  for (size_t k = 0; k < items.size(); ++k) {
+    wh[k] = items[k].w;
+    p->item_costs[k] = items[k].cost;  // target x source pairs of the item
+  }
   std::vector<SegDesc> sh(systems.size());
   std::vector<StageItem> sih, shh;
   p->stage_host.resize(systems.size());
@@ -329,6 +333,13 @@ static cudaEvent_t take_event(pawan_ctx *ctx) {
 }
 
 int launch_pairs(pawan_ctx *ctx, Plan &p, bool allow_events) {
+  return launch_pairs_range(ctx, p, 0, p.n_items, allow_events);
+}
+
+int launch_pairs_range(pawan_ctx *ctx, Plan &p, int first, int count, bool allow_events) {
+  if (first < 0 || count < 0 || first + count > p.n_items)
+    return fail(ctx, PAWAN_ERR_INVALID, "work-item range outside the plan");
+  const WorkItem *items = p.items.p + first;
   for (size_t s = 0; s < p.systems.size(); ++s)
     if (p.box_versions[s] != p.systems[s]->pack_version) {
       // another plan repacked these systems since this plan's boxes were made
@@ -345,13 +356,13 @@ int launch_pairs(pawan_ctx *ctx, Plan &p, bool allow_events) {
   }
   cudaError_t e;
   if (p.precision == PAWAN_PREC_F32)
-    e = launch_pairs_f32(p.tile.pc, p.diffusion, p.kernel, p.grid, p.items.p, p.n_items, p.segs.p,
+    e = launch_pairs_f32(p.tile.pc, p.diffusion, p.kernel, p.grid, items, count, p.segs.p,
                          ctx->d_counter, ctx->stream);
   else if (p.precision == PAWAN_PREC_F64)
-    e = launch_pairs_f64(p.tile.pc, p.diffusion, p.kernel, p.grid, p.items.p, p.n_items, p.segs.p,
+    e = launch_pairs_f64(p.tile.pc, p.diffusion, p.kernel, p.grid, items, count, p.segs.p,
                          ctx->d_counter, ctx->stream);
   else
-    e = launch_pairs_plain(p.tile.pc, p.kernel, p.grid, p.items.p, p.n_items, p.segs.p, ctx->d_counter,
+    e = launch_pairs_plain(p.tile.pc, p.kernel, p.grid, items, count, p.segs.p, ctx->d_counter,
                            ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "pair kernel launch");
   ctx->launches++;
@@ -359,7 +370,9 @@ int launch_pairs(pawan_ctx *ctx, Plan &p, bool allow_events) {
     PAWAN_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
     ctx->pending.push_back({e0, e1});
     ctx->pair_launches++;
-    ctx->pair_interactions += p.interactions;
+    double work = 0.0;
+    for (int i = first; i < first + count; ++i) work += p.item_costs[i];
+    ctx->pair_interactions += work;
   }
   return PAWAN_OK;
 }

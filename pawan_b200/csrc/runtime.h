@@ -154,6 +154,7 @@ struct Plan {
   bool diffusion = false;
   int grid = 0;
   int n_items = 0;
+  std::vector<double> item_costs;  // interactions of each work item, in launch order
   int n_stage_blocks = 0;
   double interactions = 0.0;  // sum n^2
   std::vector<int> nchunks;
@@ -182,6 +183,9 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
                bool ordered_alloc = false);
 int set_plan_dt(pawan_ctx *ctx, Plan &p, const double *dt, double dt0);
 int launch_pairs(pawan_ctx *ctx, Plan &p, bool allow_events = true);
+// The pair kernel over the plan's work items [first, first + count) only (the
+// items write disjoint partial slots, so a stage may be split over launches).
+int launch_pairs_range(pawan_ctx *ctx, Plan &p, int first, int count, bool allow_events = true);
 int launch_stage_mode(pawan_ctx *ctx, Plan &p, int mode);
 int rk4_steps(pawan_ctx *ctx, Plan &p, size_t nsteps, bool use_graph);
 int autotune_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int precision,

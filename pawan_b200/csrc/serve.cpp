@@ -18,6 +18,14 @@
 // about that long for admission while few or small active requests do not
 // pay one host round trip per step.
 //
+// A request whose single RK4 step would take longer than the target ("large",
+// decided at admission) does not step with the others: it has its own plan
+// and advances by slices of its stages' work items, the large requests taking
+// turns at about one target of work per iteration.  Small requests
+// then keep their pace beside arbitrarily large ones, as with chunked
+// prefill in language-model serving.  Its result is unchanged, bit for bit:
+// every work item writes its own partial slot whichever launch runs it.
+//
 // The engine's systems and plans take their device memory from the device's
 // memory pool in the order of the engine's stream (cudaMallocAsync /
 // cudaFreeAsync): admitting and retiring requests never synchronises the
@@ -68,6 +76,11 @@ struct Request {
   double t_submit = 0.0, t_admit = -1.0, t_done = -1.0;
   bool cancel = false;
   pawan_system *sys = nullptr;
+  // a request whose RK4 step costs more than an iteration ("large"): its own
+  // plan, and the stage / work item it has reached
+  bool large = false;
+  std::unique_ptr<Plan> plan;
+  int stage = 0, next_item = 0;
   std::vector<double> result;
 };
 
@@ -136,14 +149,40 @@ int plan_iteration(pawan_server *srv, std::vector<Request *> &act, std::unique_p
   return set_plan_dt(ctx, *plan, dts.data(), 0.0);
 }
 
-// k RK4 steps of every admitted request (replays of the plan's captured step
-// when there are several), then waits for the device.
-int run_iteration(pawan_server *srv, Plan &plan, size_t k) {
+// A slice of a large request's stage work, about `budget` interactions (at
+// least one work item per resident block of the pair kernel, so the slice
+// fills the device; on into the following stages while the budget lasts).
+// Each work item writes its own partial slot, so splitting a stage over
+// launches changes nothing in the result.  Adds the interactions done to *work.
+int large_slice(pawan_server *srv, Request *r, double budget, double *work) {
+  static const int modes[4] = {STAGE_K1, STAGE_K2, STAGE_K3, STAGE_FINAL};
   pawan_ctx *ctx = srv->ctx;
-  int st = rk4_steps(ctx, plan, k, k >= 3);
-  if (st != PAWAN_OK) return st;
-  cudaError_t e = cudaStreamSynchronize(ctx->stream);
-  if (e != cudaSuccess) return cuda_fail(ctx, e, "serving iteration");
+  Plan &p = *r->plan;
+  double used = 0.0;
+  while (r->steps_done < r->nsteps) {
+    // at least one work item per resident block (a slice fills the device)
+    int b = r->next_item;
+    double acc = 0.0;
+    while (b < p.n_items &&
+           (b - r->next_item < p.grid || used + acc + p.item_costs[b] <= budget)) {
+      acc += p.item_costs[b];
+      ++b;
+    }
+    int st = launch_pairs_range(ctx, p, r->next_item, b - r->next_item);
+    if (st != PAWAN_OK) return st;
+    used += acc;
+    r->next_item = b;
+    if (b < p.n_items) break;  // budget spent mid-stage
+    st = launch_stage_mode(ctx, p, modes[r->stage]);
+    if (st != PAWAN_OK) return st;
+    r->next_item = 0;
+    if (++r->stage == 4) {
+      r->stage = 0;
+      r->steps_done++;
+    }
+    if (used >= budget) break;
+  }
+  *work += used;
   return PAWAN_OK;
 }
 
@@ -166,6 +205,7 @@ void worker_main(pawan_server *srv) {
   cudaSetDevice(srv->ctx->device);
   std::unique_ptr<Plan> plan;
   bool set_changed = true;
+  size_t large_turn = 0;  // the large request that goes first this iteration
   for (;;) {
     std::vector<Request *> admit;
     {
@@ -232,6 +272,8 @@ void worker_main(pawan_server *srv) {
       // (the pageable particle copies were staged before system_upload returned)
       std::vector<double>().swap(r->pos);
       std::vector<double>().swap(r->vor);
+      const double target = srv->cfg.iteration_seconds > 0.0 ? srv->cfg.iteration_seconds : kIterTarget;
+      r->large = 4.0 * (double)r->n * (double)r->n / std::max(1e9, srv->rate) > target;
       srv->active.push_back(r);
       srv->stats.admitted++;
       set_changed = true;
@@ -247,13 +289,26 @@ void worker_main(pawan_server *srv) {
       act = srv->active;
     }
     if (act.empty()) continue;
+    // requests that step together, and large ones that advance by slices
+    std::vector<Request *> reg, big;
+    for (Request *r : act) (r->large ? big : reg).push_back(r);
     const auto tp0 = std::chrono::steady_clock::now();
-    int st = plan_iteration(srv, act, plan, set_changed);
+    int st = PAWAN_OK;
+    if (!reg.empty()) {
+      st = plan_iteration(srv, reg, plan, set_changed);
+    } else {
+      plan.reset();
+    }
+    for (Request *r : big) {
+      if (st != PAWAN_OK || r->plan) continue;
+      st = build_plan(srv->ctx, {r->sys}, srv->cfg.precision, srv->tile, r->plan, kServeChunkSources, true);
+      if (st == PAWAN_OK) st = set_plan_dt(srv->ctx, *r->plan, &r->dt, 0.0);
+    }
     set_changed = false;
     const auto it0 = std::chrono::steady_clock::now();
     size_t k = 0;
-    double n2 = 0.0;
-    for (Request *r : act) n2 += (double)r->n * (double)r->n;
+    double n2 = 0.0, work = 0.0;
+    for (Request *r : reg) n2 += (double)r->n * (double)r->n;
     bool inj_fail = false, inj_slow = false;
     double slow_s = 0.0;
     {
@@ -264,16 +319,34 @@ void worker_main(pawan_server *srv) {
     }
     if (inj_slow) std::this_thread::sleep_for(std::chrono::duration<double>(slow_s));
     if (st == PAWAN_OK && inj_fail) st = fail(srv->ctx, PAWAN_ERR_CUDA, "injected iteration failure");
+    if (st == PAWAN_OK && !reg.empty()) {
+      k = steps_per_iteration(srv, reg);
+      st = rk4_steps(srv->ctx, *plan, k, k >= 3);
+      work += 4.0 * n2 * (double)k;
+    }
+    if (st == PAWAN_OK && !big.empty()) {
+      // about one iteration target of work for the large requests, in turn
+      // (round robin over iterations), so that each slice is large enough to
+      // fill the device
+      const double target = srv->cfg.iteration_seconds > 0.0 ? srv->cfg.iteration_seconds : kIterTarget;
+      double budget = target * std::max(1e9, srv->rate);
+      for (size_t j = 0; j < big.size() && budget > 0.0 && st == PAWAN_OK; ++j) {
+        Request *r = big[(large_turn + j) % big.size()];
+        const double before = work;
+        st = large_slice(srv, r, budget, &work);
+        budget -= work - before;
+      }
+      large_turn = (large_turn + 1) % std::max<size_t>(1, big.size());
+    }
     if (st == PAWAN_OK) {
-      k = steps_per_iteration(srv, act);
-      st = run_iteration(srv, *plan, k);
+      cudaError_t e = cudaStreamSynchronize(srv->ctx->stream);
+      if (e != cudaSuccess) st = cuda_fail(srv->ctx, e, "serving iteration");
     }
     const auto it1 = std::chrono::steady_clock::now();
     const double busy = std::chrono::duration<double>(it1 - it0).count();
-    if (st == PAWAN_OK && busy > 0.0) {
-      // device rate of this iteration, smoothed (for the next step count)
-      const double r = 4.0 * n2 * (double)k / busy;
-      srv->rate = 0.5 * srv->rate + 0.5 * r;
+    if (st == PAWAN_OK && busy > 0.0 && work > 0.0) {
+      // device rate of this iteration, smoothed (for the next step counts)
+      srv->rate = 0.5 * srv->rate + 0.5 * work / busy;
     }
     // retire finished / cancelled requests
     std::vector<Request *> done;
@@ -283,13 +356,12 @@ void worker_main(pawan_server *srv) {
       srv->stats.busy_seconds += busy;
       srv->stats.plan_seconds += std::chrono::duration<double>(it0 - tp0).count();
       if (st != PAWAN_OK) srv->worker_error = srv->ctx->err;
-      for (Request *r : act) {
-        if (st == PAWAN_OK) {
-          r->steps_done += k;
-          srv->stats.interactions += 4.0 * (double)r->n * (double)r->n * (double)k;
-        }
-        if (st != PAWAN_OK || r->cancel || r->steps_done >= r->nsteps) done.push_back(r);
+      if (st == PAWAN_OK) {
+        for (Request *r : reg) r->steps_done += k;
+        srv->stats.interactions += work;
       }
+      for (Request *r : act)
+        if (st != PAWAN_OK || r->cancel || r->steps_done >= r->nsteps) done.push_back(r);
     }
     const auto tr0 = std::chrono::steady_clock::now();
     for (Request *r : done) {
@@ -303,6 +375,7 @@ void worker_main(pawan_server *srv) {
         if (pawan_system_get_states(r->sys, r->result.data(), r->result.size()) != PAWAN_OK)
           state = PAWAN_REQ_REJECTED;
       }
+      r->plan.reset();
       pawan_system_destroy(r->sys);
       r->sys = nullptr;
       std::lock_guard<std::mutex> lk(srv->mu);
@@ -371,8 +444,10 @@ void pawan_server_destroy(pawan_server *srv) {
   }
   srv->cv_work.notify_all();
   if (srv->worker.joinable()) srv->worker.join();
-  for (auto &kv : srv->reqs)
+  for (auto &kv : srv->reqs) {
+    kv.second->plan.reset();
     if (kv.second->sys) pawan_system_destroy(kv.second->sys);
+  }
   cudaStreamSynchronize(srv->ctx->stream);
   if (srv->pool) cudaMemPoolTrimTo(srv->pool, 0);
   pawan_ctx_destroy(srv->ctx);

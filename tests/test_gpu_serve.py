@@ -30,7 +30,8 @@ def run_alone(ctx, sc):
 
 def test_alone_and_in_the_mix_are_identical(ctx):
     scs = requests()
-    # one RK4 step per iteration, so the staggered arrivals join requests in flight
+    # a tiny iteration target: requests advance a slice of a step per iteration,
+    # so the staggered arrivals join requests in flight
     srv = Server(ctx, budget_bytes=1 << 30, iteration_seconds=1e-9)
     ids = []
     for k, sc in enumerate(scs):
@@ -216,3 +217,42 @@ def test_admission_policy_orders_the_queue(ctx, policy):
     else:
         assert t_admit_small < t_admit_big
     assert np.array_equal(outs[rc][0], run_alone(ctx, small))
+
+
+def test_large_requests_advance_by_slices_with_identical_results(ctx):
+    """With a tiny iteration target every request is "large": each advances by
+    slices of its stages' work items over many iterations.  Results are
+    bit-identical to one request alone with the ordinary path."""
+    scs = requests(k=3, seed=31)
+    srv = Server(ctx, budget_bytes=1 << 30, iteration_seconds=1e-7)
+    ids = [srv.submit_scenario(sc)[1] for sc in scs]
+    for rid in ids:
+        assert srv.wait(rid, 120)
+    outs = [srv.fetch(rid)[0] for rid in ids]
+    stats = srv.stats()
+    srv.close()
+    assert stats["completed"] == len(scs)
+    assert stats["iterations"] > 4 * sum(sc.steps for sc in scs) / len(scs)  # stages split up
+    for sc, out in zip(scs, outs):
+        assert np.array_equal(out, run_alone(ctx, sc))
+
+
+def test_small_requests_keep_their_pace_beside_a_large_one(ctx):
+    """A large request (one step far beyond the iteration target) does not hold
+    the small ones: they finish while it is still running."""
+    srv = Server(ctx, budget_bytes=8 << 30, iteration_seconds=0.002)
+    big = g.ring_pair(n_stations=2048, seed=32, steps=50)        # N = 32,768
+    rb = srv.submit_scenario(big)[1]
+    deadline = time.time() + 30
+    while srv.poll(rb) == "queued" and time.time() < deadline:
+        time.sleep(0.001)
+    small = [g.single_ring(n_stations=32, seed=33 + i, steps=5) for i in range(4)]
+    ids = [srv.submit_scenario(sc)[1] for sc in small]
+    for rid in ids:
+        assert srv.wait(rid, 60)
+    assert srv.poll(rb) == "active"
+    outs = [srv.fetch(rid)[0] for rid in ids]
+    srv.cancel(rb)
+    srv.close()
+    for sc, out in zip(small, outs):
+        assert np.array_equal(out, run_alone(ctx, sc))
