@@ -14,7 +14,9 @@ Prints one JSON line (rank 0).  `value` is device-timed throughput with the
 state resident in HBM; `e2e` is the same metric through the C ABI with host
 buffers (state H2D and D2H every step); `roofline` is the FP32 pair kernel's
 algorithmic flop rate (96 flops per interaction with diffusion) against the
-FP32 FFMA throughput measured in the same run; `cpu_baseline` is the
+FP32 FFMA throughput measured in the same run; `state_update` is the
+per-particle RK4 stage kernel's algorithmic HBM bytes per launch over its
+CUDA-event time, against the measured copy bandwidth; `cpu_baseline` is the
 reference's own OpenMP __parallel::solve (compiled from its sources) on a
 bounded sample, on this host's cores.  With --gpus N (torchrun), every rank
 runs its own ring pair (independent replicas, weak scaling); the time is the
@@ -199,6 +201,31 @@ def profile_summary() -> dict:
         except (OSError, ValueError):
             return {}
     return {}
+
+
+def hbm_peak():
+    """(GB/s, source): the measured copy bandwidth of MEASURED_PEAKS.json, else
+    the earlier measurement on these GPUs."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured: MEASURED_PEAKS.json hbm_gbs"
+    except (OSError, ValueError, KeyError, TypeError):
+        return 6650.0, "fallback: 6.65 TB/s measured earlier on these GPUs"
+
+
+def state_update_roofline(prof_stage: dict) -> dict:
+    """HBM roofline of the per-particle stage kernel (RK4 stage update and
+    repack) over the timed steps: algorithmic bytes / CUDA-event time."""
+    peak, src = hbm_peak()
+    n = max(1, prof_stage["stage_launches"])
+    ms = prof_stage["stage_ms"] / n
+    gbs = prof_stage["stage_bytes"] / n / (ms * 1e-3) / 1e9 if ms > 0 else None
+    return {"kernel": "stage_kernel", "bound": "hbm", "launches": prof_stage["stage_launches"],
+            "ms_per_launch": ms, "bytes_per_launch": prof_stage["stage_bytes"] / n,
+            "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": (gbs / peak) if gbs else None,
+            "peak_source": src,
+            "note": "the chunk partials it reads were just written by the pair kernel and are "
+                    "partly L2-resident, so frac can exceed 1"}
 
 
 def traffic_from_profiles():
@@ -425,6 +452,7 @@ def run_pawan(args, rk: Ranks):
     ctx.synchronize()
     launches = ctx.launch_count - launches0
     prof = ctx.profile_read()
+    prof_stage = ctx.profile_stage()
     ctx.profile(False)
     clk = clocks.stop()
     clk["compute_processes"] = gpu_processes(gpu_index(rk.local))
@@ -460,7 +488,8 @@ def run_pawan(args, rk: Ranks):
                                  "utilisation: ncu FMA-pipe activity in executed_ncu",
                          "executed_ncu": {k: profile_summary().get(k) for k in
                                           ("fma_pipe_active", "fma_pipe_lane_ops_per_interaction",
-                                           "thread_instructions_per_interaction")}}}
+                                           "thread_instructions_per_interaction")}},
+            "state_update": state_update_roofline(prof_stage)}
 
     if not args.quick:
         # plain FP64 comparator and tuned FP64 on the same workload: one RHS each

@@ -81,6 +81,11 @@ int pawan_ctx_profile(pawan_ctx *ctx, int enable);
  * pair launches, and pair interactions counted as N^2 per solve per launch. */
 int pawan_ctx_profile_read(pawan_ctx *ctx, double *pair_ms, unsigned long long *pair_launches,
                            double *pair_interactions);
+/* The same for the per-particle stage kernel (RK4 stage update and repack):
+ * summed time (ms), launches, and algorithmic HBM bytes (what each launch must
+ * read and write: chunk partials, FP64 state vectors, packed tile data). */
+int pawan_ctx_profile_stage(pawan_ctx *ctx, double *stage_ms, unsigned long long *stage_launches,
+                            double *stage_bytes);
 /* Timing marks on the context's stream (CUDA events, slots 0..15) and the
  * device time between two of them, in ms (waits for the later mark). */
 int pawan_ctx_mark(pawan_ctx *ctx, int slot);

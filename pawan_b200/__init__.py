@@ -115,6 +115,7 @@ _SIGS = {
     "pawan_system_influence": (ctypes.c_int, [_vp, _dp, ctypes.c_size_t]),
     "pawan_shard_size": (ctypes.c_size_t, [ctypes.c_size_t, ctypes.c_int]),
     "pawan_system_set_kernel": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "pawan_ctx_profile_stage": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_ulonglong), _dp]),
     "pawan_system_integrate": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_size_t, ctypes.c_char_p,
                                               ctypes.c_int]),
     "pawan_system_integrate_file": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_size_t, _vp, ctypes.c_int]),
@@ -260,6 +261,14 @@ class Context:
         self.check(self._lib.pawan_ctx_profile_read(self._h, ctypes.byref(ms), ctypes.byref(n),
                                                     ctypes.byref(inter)))
         return {"pair_ms": ms.value, "pair_launches": n.value, "pair_interactions": inter.value}
+
+    def profile_stage(self) -> dict:
+        """Stage-kernel totals since profiling was enabled: ms, launches, and
+        algorithmic HBM bytes."""
+        ms, n, b = ctypes.c_double(), ctypes.c_ulonglong(), ctypes.c_double()
+        self.check(self._lib.pawan_ctx_profile_stage(self._h, ctypes.byref(ms), ctypes.byref(n),
+                                                     ctypes.byref(b)))
+        return {"stage_ms": ms.value, "stage_launches": n.value, "stage_bytes": b.value}
 
     def mark(self, slot: int):
         self.check(self._lib.pawan_ctx_mark(self._h, int(slot)))

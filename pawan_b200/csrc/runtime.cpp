@@ -384,10 +384,49 @@ static void note_repack(Plan &p) {
   }
 }
 
+// Algorithmic HBM bytes of one stage launch: per particle the chunk partials
+// (or the gathered rates of a sharded system), the FP64 state vectors the mode
+// reads and writes, radius and volume, and the 128 bytes of packed FP32 / FP64
+// tile data; 32 bytes of bounding box per tile.
+static double stage_bytes(const Plan &p, int mode) {
+  double total = 0.0;
+  for (size_t s = 0; s < p.systems.size(); ++s) {
+    const pawan_system *y = p.systems[s];
+    const double n = (double)y->n;
+    const double rates = y->shard.active ? 48.0 : 48.0 * (double)p.nchunks[s];
+    const double pack = 16.0 + 128.0 + 32.0 / (double)p.tile.pc.tb;
+    double per = 0.0;
+    switch (mode) {
+      case STAGE_RATES: per = rates + 48.0; break;
+      case STAGE_K1: case STAGE_K2: per = rates + 48.0 + 96.0 + pack; break;
+      case STAGE_K3: per = rates + 96.0 + 96.0 + pack; break;
+      case STAGE_FINAL: per = rates + 144.0 + 48.0 + pack; break;
+      case STAGE_EULER: per = rates + 48.0 + 48.0 + pack; break;
+      case STAGE_PACK: per = 48.0 + pack; break;
+      default: per = 0.0;
+    }
+    total += n * per;
+  }
+  return total;
+}
+
 int launch_stage_mode(pawan_ctx *ctx, Plan &p, int mode) {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ctx->profile) {
+    e0 = take_event(ctx);
+    e1 = take_event(ctx);
+    if (!e0 || !e1) return fail(ctx, PAWAN_ERR_CUDA, "cannot create profiling events");
+    PAWAN_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
+  }
   cudaError_t e = launch_stage(mode, p.n_stage_blocks, p.stage_items.p, p.stage_descs.p, ctx->stream);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "stage kernel launch");
   ctx->launches++;
+  if (e0) {
+    PAWAN_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
+    ctx->stage_pending.push_back({e0, e1});
+    ctx->stage_launches++;
+    ctx->stage_bytes += stage_bytes(p, mode);
+  }
   if (mode != STAGE_RATES) note_repack(p);
   return PAWAN_OK;
 }
@@ -732,10 +771,11 @@ void pawan_ctx_destroy(pawan_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  for (auto &pr : ctx->pending) {
-    cudaEventDestroy(pr.first);
-    cudaEventDestroy(pr.second);
-  }
+  for (auto *pend : {&ctx->pending, &ctx->stage_pending})
+    for (auto &pr : *pend) {
+      cudaEventDestroy(pr.first);
+      cudaEventDestroy(pr.second);
+    }
   for (auto e : ctx->event_pool) cudaEventDestroy(e);
   for (auto e : ctx->marks)
     if (e) cudaEventDestroy(e);
@@ -769,14 +809,19 @@ unsigned long long pawan_ctx_launch_count(const pawan_ctx *ctx) {
 int pawan_ctx_profile(pawan_ctx *ctx, int enable) {
   CHECK_CTX(ctx);
   PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  for (auto &pr : ctx->pending) {
-    ctx->event_pool.push_back(pr.first);
-    ctx->event_pool.push_back(pr.second);
+  for (auto *pend : {&ctx->pending, &ctx->stage_pending}) {
+    for (auto &pr : *pend) {
+      ctx->event_pool.push_back(pr.first);
+      ctx->event_pool.push_back(pr.second);
+    }
+    pend->clear();
   }
-  ctx->pending.clear();
   ctx->pair_ms = 0.0;
   ctx->pair_launches = 0;
   ctx->pair_interactions = 0.0;
+  ctx->stage_ms = 0.0;
+  ctx->stage_launches = 0;
+  ctx->stage_bytes = 0.0;
   ctx->profile = enable != 0;
   return PAWAN_OK;
 }
@@ -796,6 +841,24 @@ int pawan_ctx_profile_read(pawan_ctx *ctx, double *pair_ms, unsigned long long *
   if (pair_ms) *pair_ms = ctx->pair_ms;
   if (pair_launches) *pair_launches = ctx->pair_launches;
   if (pair_interactions) *pair_interactions = ctx->pair_interactions;
+  return PAWAN_OK;
+}
+
+int pawan_ctx_profile_stage(pawan_ctx *ctx, double *stage_ms, unsigned long long *stage_launches,
+                            double *stage_bytes) {
+  CHECK_CTX(ctx);
+  PAWAN_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (auto &pr : ctx->stage_pending) {
+    float ms = 0.f;
+    PAWAN_CUDA(ctx, cudaEventElapsedTime(&ms, pr.first, pr.second));
+    ctx->stage_ms += ms;
+    ctx->event_pool.push_back(pr.first);
+    ctx->event_pool.push_back(pr.second);
+  }
+  ctx->stage_pending.clear();
+  if (stage_ms) *stage_ms = ctx->stage_ms;
+  if (stage_launches) *stage_launches = ctx->stage_launches;
+  if (stage_bytes) *stage_bytes = ctx->stage_bytes;
   return PAWAN_OK;
 }
 

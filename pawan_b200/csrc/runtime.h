@@ -95,6 +95,11 @@ struct pawan_ctx {
   double pair_ms = 0.0;
   unsigned long long pair_launches = 0;
   double pair_interactions = 0.0;
+  // the same for the per-particle stage kernel, with its algorithmic bytes
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> stage_pending;
+  double stage_ms = 0.0;
+  unsigned long long stage_launches = 0;
+  double stage_bytes = 0.0;
   cudaEvent_t marks[16] = {};
   void *flush_buf = nullptr;
   size_t flush_bytes = 0;

@@ -21,6 +21,16 @@
 namespace pawan {
 namespace {
 
+// Partial chunks loaded per batch, and blocks per SM the register budget is
+// held to: a segment of 131,072 particles is 512 blocks of 256, one wave at
+// four blocks per SM on 148 SMs.  The descriptor is read through a reference
+// (uniform, L1-cached) rather than copied, which is what frees the registers.
+// Measured at N = 131,072 with 16 chunks: batch 1 or 2 at 64 registers
+// 28.6 us per launch; batch 3 or 4 (spilling at 64, or 80-85 registers and
+// three blocks per SM) 30-34 us; batch 8 at 134 registers 37 us.
+constexpr int kStageChunkBatch = 2;
+constexpr int kStageMinBlocks = 4;
+
 // Packs one particle: FP32 hi/lo pairs of the position relative to the
 // system's origin and of the strength, plus the FP64 copies.  Returns the hi
 // position and h = s^2/2 for the tile's bounding box.
@@ -77,10 +87,10 @@ __device__ __forceinline__ void tile_boxes(const StageDesc &d, int l0, float4 p,
 }
 
 template <int MODE>
-__global__ void __launch_bounds__(kStageThreads)
+__global__ void __launch_bounds__(kStageThreads, kStageMinBlocks)
     stage_kernel(const StageItem *__restrict__ items, const StageDesc *__restrict__ descs) {
   const StageItem it = items[blockIdx.x];
-  const StageDesc d = descs[it.seg];
+  const StageDesc &d = descs[it.seg];
   const int l = it.l0 + threadIdx.x;
   const bool has = l < d.n;
   const size_t n = (size_t)d.n;
@@ -99,12 +109,28 @@ __global__ void __launch_bounds__(kStageThreads)
 #pragma unroll
       for (int k = 0; k < 6; ++k) r[k] = g[(size_t)k * S];
     } else {
+      // Chunks are summed in order (r = c0, then r += c1, c2, ...), but
+      // loaded kStageChunkBatch at a time, the last batch partly, so that
+      // each thread keeps 6 x kStageChunkBatch loads in flight: the kernel is
+      // bound by memory latency, not by its few adds.  The partials are read
+      // once; streaming loads keep them from evicting the state from L2.
+      for (int c0 = 0; c0 < d.nchunks; c0 += kStageChunkBatch) {
+        double v[kStageChunkBatch][6];
 #pragma unroll
-      for (int k = 0; k < 6; ++k) r[k] = d.partial[(size_t)k * n + l];
-      for (int c = 1; c < d.nchunks; ++c) {
-        const double *p = d.partial + (size_t)c * 6 * n + l;
+        for (int u = 0; u < kStageChunkBatch; ++u) {
+          if (c0 + u < d.nchunks) {
+            const double *p = d.partial + (size_t)(c0 + u) * 6 * n + l;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) r[k] = __dadd_rn(r[k], p[(size_t)k * n]);
+            for (int k = 0; k < 6; ++k) v[u][k] = __ldcs(p + (size_t)k * n);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kStageChunkBatch; ++u) {
+          if (c0 + u < d.nchunks) {
+#pragma unroll
+            for (int k = 0; k < 6; ++k) r[k] = (c0 + u == 0) ? v[u][k] : __dadd_rn(r[k], v[u][k]);
+          }
+        }
       }
     }
   }
