@@ -156,6 +156,15 @@ int pawan_system_kinetic_energy(pawan_system *sys, double *ke);
  * influence-matrix path of __resolve::rebuild (src/resolve/resolve.cpp:10-57)
  * calls it once per state component. */
 int pawan_system_influence(pawan_system *sys, double *field, size_t size);
+/* The vorticity field of ncols strength vectors at once, over the system's
+ * current positions and radii: alpha holds ncols blocks of N x 3 doubles
+ * (wake order, the rows of every wake's _vorticity), field receives the same
+ * shape (size = ncols * 3N for both).  These are the influence-matrix columns
+ * of __resolve::rebuild (resolve.cpp:19-31), which differ only in strength;
+ * each column is bit-identical to pawan_system_influence with that strength.
+ * The system's own strengths are not changed. */
+int pawan_system_influence_columns(pawan_system *sys, size_t ncols, const double *alpha,
+                                   double *field, size_t size);
 /* The protected __interaction::_nu (interaction.h:24). */
 int pawan_system_set_nu(pawan_system *sys, double nu);
 int pawan_system_set_precision(pawan_system *sys, int precision);

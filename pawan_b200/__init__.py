@@ -113,6 +113,7 @@ _SIGS = {
     "pawan_system_diagnose": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
     "pawan_system_kinetic_energy": (ctypes.c_int, [_vp, _dp]),
     "pawan_system_influence": (ctypes.c_int, [_vp, _dp, ctypes.c_size_t]),
+    "pawan_system_influence_columns": (ctypes.c_int, [_vp, ctypes.c_size_t, _dp, _dp, ctypes.c_size_t]),
     "pawan_shard_size": (ctypes.c_size_t, [ctypes.c_size_t, ctypes.c_int]),
     "pawan_system_set_kernel": (ctypes.c_int, [_vp, ctypes.c_int]),
     "pawan_ctx_profile_stage": (ctypes.c_int, [_vp, _dp, ctypes.POINTER(ctypes.c_ulonglong), _dp]),
@@ -414,6 +415,19 @@ class System:
         ``__interaction::resolve()`` / ``influence()``."""
         k = np.empty((self.n, 3))
         self.ctx.check(self._lib.pawan_system_influence(self._h, _p(k), k.size))
+        return k
+
+    def influence_columns(self, alpha) -> np.ndarray:
+        """Vorticity field of several strength vectors over the current
+        positions and radii: ``alpha`` is (C, N, 3), the result (C, N, 3).
+        The influence-matrix columns of ``__resolve::rebuild``, one launch per
+        group of columns; the system's own strengths are unchanged."""
+        a = np.ascontiguousarray(alpha, dtype=np.float64)
+        if a.ndim != 3 or a.shape[1:] != (self.n, 3):
+            raise ValueError(f"alpha must be (C, {self.n}, 3)")
+        k = np.empty_like(a)
+        self.ctx.check(self._lib.pawan_system_influence_columns(self._h, a.shape[0], _p(a), _p(k),
+                                                                 k.size))
         return k
 
     def set_nu(self, nu: float):

@@ -21,6 +21,14 @@
 // one rsqrt per pair; the path is small next to the interaction (it is run
 // once per influence-matrix column), so FP64 throughout keeps the resolve's
 // linear solve as accurate as the reference's.
+//
+// The columns kernel evaluates the field of many strength vectors over the
+// same positions and radii at once -- the influence-matrix columns of
+// __resolve::rebuild (resolve.cpp:19-31), which differ only in alpha.  Z of a
+// pair is formed once and applied to kColGroup columns (3 FMAs each), so a
+// column costs 3 FMAs per pair instead of ~20 operations.  Both kernels form
+// Z with the same function and accumulate with explicit FMAs in source order,
+// so a column of the batched kernel is bit-identical to a single-column launch.
 #include "device.cuh"
 #include "kernels.h"
 
@@ -28,6 +36,31 @@ namespace pawan {
 namespace {
 
 constexpr int kInfThreads = 128;
+constexpr int kColGroup = kInfluenceColumnGroup;  // 3 x 8 FP64 accumulators per thread
+
+// Z(rho_ij, sigma_ij) for target i (position ri, hi = s_i^2 / 2) and source
+// j (rj = position, smoothing radius); operations written out so that every
+// kernel rounds them the same way.
+template <int KERN>
+__device__ __forceinline__ double pair_z(const double4 ri, double hi, const double4 rj) {
+  const double dx = __dsub_rn(ri.x, rj.x), dy = __dsub_rn(ri.y, rj.y), dz = __dsub_rn(ri.z, rj.z);
+  const double rho2 = __fma_rn(dz, dz, __fma_rn(dy, dy, __dmul_rn(dx, dx)));
+  const double sig2 = __fma_rn(0.5 * rj.w, rj.w, hi);
+  if (KERN == KERNEL_GAUSSIAN) {
+    const double cg = 0.06349363593424096978;  // (2 pi)^-1.5
+    const double is = rsqrt(sig2);
+    const double is2 = __dmul_rn(is, is);
+    return __dmul_rn(__dmul_rn(exp(-0.5 * __dmul_rn(rho2, is2)), __dmul_rn(is2, is)), cg);
+  } else {
+    const double c = 1.875 * kInvPi;  // 15 / (8 pi)
+    const double w = rsqrt(__dadd_rn(rho2, sig2));
+    const double w2 = __dmul_rn(w, w);
+    const double u = __dmul_rn(sig2, w2);
+    const double u2 = __dmul_rn(u, u);
+    const double u6 = __dmul_rn(__dmul_rn(u2, u2), u2);
+    return __dmul_rn(__dmul_rn(c, u6), __dmul_rn(w2, w));
+  }
+}
 
 template <int KERN>
 __global__ void __launch_bounds__(kInfThreads)
@@ -39,9 +72,7 @@ __global__ void __launch_bounds__(kInfThreads)
   const int i = blockIdx.x * kInfThreads + tid;
   const bool valid = i < n;
   const double4 ri = valid ? pos[i] : make_double4(0.0, 0.0, 0.0, 1.0);
-  const double hi = 0.5 * ri.w * ri.w;
-  const double c = 1.875 * kInvPi;  // 15 / (8 pi)
-  const double cg = 0.06349363593424096978;  // (2 pi)^-1.5
+  const double hi = __dmul_rn(0.5 * ri.w, ri.w);
   double kx = 0.0, ky = 0.0, kz = 0.0;
   for (int ts = 0; ts < n; ts += kInfThreads) {
     __syncthreads();
@@ -53,25 +84,11 @@ __global__ void __launch_bounds__(kInfThreads)
     __syncthreads();
     const int cnt = min(kInfThreads, n - ts);
     for (int jj = 0; jj < cnt; ++jj) {
-      const double4 rj = sp[jj], aj = sv[jj];
-      const double dx = ri.x - rj.x, dy = ri.y - rj.y, dz = ri.z - rj.z;
-      const double rho2 = dx * dx + dy * dy + dz * dz;
-      const double sig2 = hi + 0.5 * rj.w * rj.w;
-      double z;
-      if (KERN == KERNEL_GAUSSIAN) {
-        const double is = rsqrt(sig2);
-        z = exp(-0.5 * rho2 * is * is) * (is * is * is) * cg;
-      } else {
-        const double w = rsqrt(rho2 + sig2);
-        const double w2 = w * w;
-        const double u = sig2 * w2;
-        const double u2 = u * u;
-        const double u6 = u2 * u2 * u2;
-        z = c * u6 * w2 * w;
-      }
-      kx += z * aj.x;
-      ky += z * aj.y;
-      kz += z * aj.z;
+      const double4 aj = sv[jj];
+      const double z = pair_z<KERN>(ri, hi, sp[jj]);
+      kx = __fma_rn(z, aj.x, kx);
+      ky = __fma_rn(z, aj.y, ky);
+      kz = __fma_rn(z, aj.z, kz);
     }
   }
   if (valid) {
@@ -81,7 +98,72 @@ __global__ void __launch_bounds__(kInfThreads)
   }
 }
 
+// Grid: (target blocks, column groups).  cols and field are ncols blocks of
+// N x 3 doubles (column c, particle j, component k at (c*N + j)*3 + k).
+template <int KERN>
+__global__ void __launch_bounds__(kInfThreads)
+    influence_columns_kernel(int n, int ncols, const double4 *__restrict__ pos,
+                             const double *__restrict__ cols, double *__restrict__ field) {
+  __shared__ double4 sp[kInfThreads];
+  __shared__ double sa[kColGroup][3 * kInfThreads];
+  const int tid = threadIdx.x;
+  const int i = blockIdx.x * kInfThreads + tid;
+  const int c0 = blockIdx.y * kColGroup;
+  const int nc = min(kColGroup, ncols - c0);
+  const bool valid = i < n;
+  const double4 ri = valid ? pos[i] : make_double4(0.0, 0.0, 0.0, 1.0);
+  const double hi = __dmul_rn(0.5 * ri.w, ri.w);
+  double k[kColGroup][3];
+#pragma unroll
+  for (int c = 0; c < kColGroup; ++c) k[c][0] = k[c][1] = k[c][2] = 0.0;
+  for (int ts = 0; ts < n; ts += kInfThreads) {
+    __syncthreads();
+    const int cnt = min(kInfThreads, n - ts);
+    if (tid < cnt) sp[tid] = pos[ts + tid];
+    for (int c = 0; c < nc; ++c) {
+      const double *src = cols + ((size_t)(c0 + c) * n + ts) * 3;
+      for (int e = tid; e < 3 * cnt; e += kInfThreads) sa[c][e] = src[e];
+    }
+    __syncthreads();
+    for (int jj = 0; jj < cnt; ++jj) {
+      const double z = pair_z<KERN>(ri, hi, sp[jj]);
+#pragma unroll
+      for (int c = 0; c < kColGroup; ++c) {
+        if (c < nc) {
+          k[c][0] = __fma_rn(z, sa[c][3 * jj], k[c][0]);
+          k[c][1] = __fma_rn(z, sa[c][3 * jj + 1], k[c][1]);
+          k[c][2] = __fma_rn(z, sa[c][3 * jj + 2], k[c][2]);
+        }
+      }
+    }
+  }
+  if (valid) {
+#pragma unroll
+    for (int c = 0; c < kColGroup; ++c) {
+      if (c < nc) {
+        double *o = field + ((size_t)(c0 + c) * n + i) * 3;
+        o[0] = k[c][0];
+        o[1] = k[c][1];
+        o[2] = k[c][2];
+      }
+    }
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_influence_columns(int n, int ncols, int kernel, const double4 *pos64,
+                                     const double *cols, double *field, cudaStream_t s) {
+  if (n <= 0 || ncols <= 0) return cudaSuccess;
+  const int groups = (ncols + kColGroup - 1) / kColGroup;
+  if (groups > 65535) return cudaErrorInvalidValue;
+  const dim3 grid((n + kInfThreads - 1) / kInfThreads, groups);
+  if (kernel == KERNEL_GAUSSIAN)
+    influence_columns_kernel<KERNEL_GAUSSIAN><<<grid, kInfThreads, 0, s>>>(n, ncols, pos64, cols, field);
+  else
+    influence_columns_kernel<KERNEL_HIGHORDER><<<grid, kInfThreads, 0, s>>>(n, ncols, pos64, cols, field);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_influence(int n, int kernel, const double4 *pos64, const double4 *vor64,
                              double *field, cudaStream_t s) {

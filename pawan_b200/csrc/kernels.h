@@ -63,6 +63,14 @@ cudaError_t launch_diagnostics(int n, int kernel, const double4 *pos64, const do
 // Vorticity field (FP64) of one system: field[3i..3i+2] = sum_j Z_ij alpha_j.
 cudaError_t launch_influence(int n, int kernel, const double4 *pos64, const double4 *vor64,
                              double *field, cudaStream_t s);
+// Columns per block of the columns kernel; a launch covers at most
+// 65,535 x kInfluenceColumnGroup columns (the grid's y extent).
+constexpr int kInfluenceColumnGroup = 8;
+// The same for ncols strength vectors over one set of positions and radii:
+// cols and field are ncols blocks of N x 3 doubles; column c of field is
+// bit-identical to launch_influence with vor64 = column c of cols.
+cudaError_t launch_influence_columns(int n, int ncols, int kernel, const double4 *pos64,
+                                     const double *cols, double *field, cudaStream_t s);
 
 // Throughput probes: FP32 FFMA and FP64 DFMA chains.  flops = launched FMAs * 2.
 cudaError_t launch_ffma_peak(int blocks, int threads, int iters, float *sink, cudaStream_t s);

@@ -1054,6 +1054,49 @@ int pawan_system_influence(pawan_system *sys, double *field, size_t size) {
   return PAWAN_OK;
 }
 
+// Device scratch bound of pawan_system_influence_columns (strength columns
+// plus their fields): larger requests run in several launches.
+constexpr size_t kInfluenceColumnBytes = size_t(256) << 20;
+constexpr size_t kMaxInfluenceColumnsPerLaunch = size_t(65535) * kInfluenceColumnGroup;
+
+static int influence_columns(pawan_system *sys, size_t ncols, const double *alpha, double *field,
+                             DBuf<double> &cols, DBuf<double> &out) {
+  pawan_ctx *ctx = sys->ctx;
+  const size_t per = 3 * sys->n;
+  const size_t fit = std::max<size_t>(1, kInfluenceColumnBytes / (2 * per * sizeof(double)));
+  const size_t chunk = std::min(ncols, std::min(fit, kMaxInfluenceColumnsPerLaunch));
+  PAWAN_CUDA(ctx, cols.alloc(chunk * per));
+  PAWAN_CUDA(ctx, out.alloc(chunk * per));
+  for (size_t c0 = 0; c0 < ncols; c0 += chunk) {
+    const size_t nc = std::min(chunk, ncols - c0);
+    PAWAN_CUDA(ctx, cudaMemcpyAsync(cols.p, alpha + c0 * per, nc * per * sizeof(double),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+    PAWAN_CUDA(ctx, launch_influence_columns((int)sys->n, (int)nc, sys->kernel, sys->pos64.p, cols.p,
+                                             out.p, ctx->stream));
+    ctx->launches++;
+    PAWAN_CUDA(ctx, cudaMemcpyAsync(field + c0 * per, out.p, nc * per * sizeof(double),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  return PAWAN_OK;
+}
+
+int pawan_system_influence_columns(pawan_system *sys, size_t ncols, const double *alpha,
+                                   double *field, size_t size) {
+  CHECK_SYS(sys);
+  pawan_ctx *ctx = sys->ctx;
+  if (ncols == 0) return fail(ctx, PAWAN_ERR_INVALID, "ncols must be positive");
+  if (!alpha || !field || size / ncols != 3 * sys->n || size % ncols != 0)
+    return fail(ctx, PAWAN_ERR_INVALID, "alpha and field must hold ncols * 3N doubles");
+  if (!sys->has_particles) return fail(ctx, PAWAN_ERR_STATE, "particles not set");
+  DBuf<double> cols, out;
+  const int st = influence_columns(sys, ncols, alpha, field, cols, out);
+  // the scratch is freed on return: wait for the copies and launches first
+  const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  if (st != PAWAN_OK) return st;
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "influence columns");
+  return PAWAN_OK;
+}
+
 size_t pawan_shard_size(size_t n, int world) {
   if (world < 1 || n == 0) return 0;
   const size_t per = (n + (size_t)world - 1) / (size_t)world;

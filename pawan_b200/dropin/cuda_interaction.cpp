@@ -1,6 +1,7 @@
 /* Drop-in GPU interaction for pawan; see cuda_interaction.h. */
 #include "cuda_interaction.h"
 
+#include <algorithm>
 #include <cstring>
 
 namespace pawan {
@@ -143,6 +144,39 @@ void __cuda::influence() {
   }
 }
 
+size_t __cuda::numParticles() const {
+  size_t n = 0;
+  for (auto *w : _wakes) n += w->_numParticles;
+  return n;
+}
+
+void __cuda::gatherPositions(double *out) const {
+  for (auto *w : _wakes) {
+    gather_rows(w->_position, out);
+    out += 3 * w->_numParticles;
+  }
+}
+
+void __cuda::gatherVorticity(double *out) const {
+  for (auto *w : _wakes) {
+    gather_rows(w->_vorticity, out);
+    out += 3 * w->_numParticles;
+  }
+}
+
+void __cuda::scatterField(const double *field) {
+  for (auto *w : _wakes) {
+    scatter_rows(field, w->_vorticityfield);
+    field += 3 * w->_numParticles;
+  }
+}
+
+void __cuda::influenceColumns(size_t ncols, const double *alpha, double *field) {
+  ensure_system();
+  check(pawan_system_influence_columns(_sys, ncols, alpha, field, ncols * 3 * numParticles()),
+        "influence_columns");
+}
+
 void __cuda::diagnose() {
   upload();
   double out[11];
@@ -167,6 +201,112 @@ double __cuda::kineticEnergy() {
   check(pawan_system_kinetic_energy(_sys, &ke), "kinetic_energy");
   _kineticEnergy = ke;
   return ke;
+}
+
+namespace {
+// Host memory bound of one batch of resolve columns (strengths + fields).
+constexpr size_t kResolveBatchBytes = size_t(512) << 20;
+
+struct ResolveBuffers {
+  gsl_vector *states = nullptr, *vrxfield = nullptr, *result = nullptr;
+  gsl_matrix *influence = nullptr;
+  gsl_permutation *p = nullptr;
+  FILE *f = nullptr;
+  ~ResolveBuffers() {
+    if (f) std::fclose(f);
+    if (p) gsl_permutation_free(p);
+    if (influence) gsl_matrix_free(influence);
+    if (result) gsl_vector_free(result);
+    if (vrxfield) gsl_vector_free(vrxfield);
+    if (states) gsl_vector_free(states);
+  }
+};
+}  // namespace
+
+void __cuda_resolve::rebuild(__interaction *IN, __io *IO) {
+  __cuda *C = dynamic_cast<__cuda *>(IN);
+  if (!C) {
+    __resolve::rebuild(IN, IO);
+    return;
+  }
+  const size_t S = IN->_size;
+  const size_t per = 3 * C->numParticles();
+  ResolveBuffers b;
+  b.states = gsl_vector_calloc(S);
+  b.influence = gsl_matrix_calloc(S, S);
+  b.f = IO->create_binary_file(".wakeinfluence");
+  if (!b.f) throw std::runtime_error("pawan_b200: cannot create the .wakeinfluence file");
+  double t = 0.0;
+  std::fwrite(&t, sizeof(double), 1, b.f);
+  IN->write(b.f);
+  IN->getStates(b.states);
+  std::vector<double> orig(S);
+  for (size_t i = 0; i < S; ++i) orig[i] = gsl_vector_get(b.states, i);
+  const double tStart = TIME();
+  OUT("Calculating influence matrix of all particles.");
+  const size_t batch = std::max<size_t>(1, kResolveBatchBytes / (2 * per * sizeof(double)));
+  std::vector<double> base(per), pos(per), alpha, field;
+  size_t i = 0;
+  while (i < S) {
+    // Columns [first, i): each sets its state entry to 1 (the reference's
+    // loop, resolve.cpp:19-31), while the positions stay those of `first`.
+    const size_t first = i;
+    alpha.clear();
+    while (i < S && i - first < batch) {
+      gsl_vector_set(b.states, i, 1.0);
+      IN->setStates(b.states);
+      C->gatherPositions(pos.data());
+      if (i == first) {
+        base = pos;
+      } else if (std::memcmp(pos.data(), base.data(), per * sizeof(double)) != 0) {
+        gsl_vector_set(b.states, i, orig[i]);  // column i starts the next batch
+        break;
+      }
+      alpha.resize((i - first + 1) * per);
+      C->gatherVorticity(alpha.data() + (i - first) * per);
+      OUT("\ti", i);
+      gsl_vector_set(b.states, i, 0.0);
+      t += 1.0;
+      std::fwrite(&t, sizeof(double), 1, b.f);
+      IN->write(b.f);  // x, alpha, s: what the reference writes after the column's resolve
+      ++i;
+    }
+    const size_t nc = i - first;
+    // Replay the columns' states: the positions of the batch go to the device
+    // with the first, and each column's field is read through getRates with the
+    // state vector exactly as the reference has it at that column.
+    for (size_t j = first; j < i; ++j) gsl_vector_set(b.states, j, orig[j]);
+    gsl_vector_set(b.states, first, 1.0);
+    IN->setStates(b.states);
+    C->upload();
+    field.resize(nc * per);
+    C->influenceColumns(nc, alpha.data(), field.data());
+    for (size_t j = first; j < i; ++j) {
+      if (j > first) {
+        gsl_vector_set(b.states, j, 1.0);
+        IN->setStates(b.states);
+      }
+      C->scatterField(field.data() + (j - first) * per);
+      gsl_vector_view column = gsl_matrix_column(b.influence, j);
+      IN->getRates(&column.vector);
+      gsl_vector_set(b.states, j, 0.0);
+    }
+  }
+  std::fclose(b.f);
+  b.f = nullptr;
+  OUT("Calculating expected vorticity field.");
+  b.vrxfield = gsl_vector_calloc(S);
+  IN->getIdealRates(b.vrxfield);
+  OUT("Solving vorticity strengths.");
+  b.result = gsl_vector_calloc(S);
+  int s = 0;
+  b.p = gsl_permutation_alloc(S);
+  gsl_linalg_LU_decomp(b.influence, b.p, &s);
+  gsl_linalg_LU_solve(b.influence, b.p, b.vrxfield, b.result);
+  const double tEnd = TIME();
+  OUT("Total Time (s)", tEnd - tStart);
+  OUT("Applying new vorticity strengths.");
+  IN->setStates(b.result);
 }
 
 void __cuda_rk4::integrate(__system *S, __io *IO) {

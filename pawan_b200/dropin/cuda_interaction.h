@@ -27,6 +27,7 @@
 #include "pawan_b200.h"
 #include "src/integration/rk4.h"
 #include "src/interaction/interaction.h"
+#include "src/resolve/resolve.h"
 #include "src/wake/wake.h"
 
 namespace pawan {
@@ -56,6 +57,16 @@ class __cuda : public __interaction {
   /* Copies the device state back into the wakes' _position / _vorticity. */
   void download();
   pawan_system *device_system() { return _sys; }
+  /* Particles over all wakes; their current positions / vorticities as N x 3
+   * rows in wake order; a field of that shape written into every wake's
+   * _vorticityfield. */
+  size_t numParticles() const;
+  void gatherPositions(double *out) const;
+  void gatherVorticity(double *out) const;
+  void scatterField(const double *field);
+  /* The vorticity field of ncols strength vectors (ncols x N x 3, wake order)
+   * over the positions and radii last uploaded. */
+  void influenceColumns(size_t ncols, const double *alpha, double *field);
 
  protected:
   /* The whole-solve hook (interaction.h:106): every wake pair in one launch. */
@@ -76,6 +87,22 @@ class __cuda : public __interaction {
   bool _particles_uploaded = false;
   void ensure_system();
   void check(int status, const char *what) const;
+};
+
+/* pawan::__cuda_resolve is a drop-in for __resolve (src/resolve/resolve.h):
+ * rebuild() does what the reference's does (resolve.cpp:10-57) -- the same
+ * .wakeinfluence frames, the same influence matrix filled column by column
+ * through the system's setStates / getRates, the same GSL LU solve, and
+ * setStates of the result -- but the vorticity fields of the columns are
+ * evaluated on the device in batches: consecutive columns whose states put
+ * the particles at the same positions (every column of a __vring, whose state
+ * is its strengths) go to the GPU in one call instead of one solve each.
+ * rebuild() is not virtual in the reference, so call it through a
+ * __cuda_resolve; an interaction that is not a __cuda goes through the
+ * reference's rebuild. */
+class __cuda_resolve : public __resolve {
+ public:
+  void rebuild(__interaction *IN, __io *IO);
 };
 
 class __cuda_rk4 : public __rk4 {

@@ -4,6 +4,7 @@
 // the reference's __interaction.  Built by `make -C oracle dropin` into
 // oracle/_ref/libpawan_dropin.so; used only by tests/test_gpu_dropin.py.
 #include <cstdio>
+#include <string>
 #include <vector>
 
 #include "pawan_b200/dropin/cuda_interaction.h"
@@ -284,6 +285,52 @@ int dropin_vring_resolve(double radius, double core, int layers, double *gpu, do
     delete R;
     delete Vg;
     delete Vc;
+    return 0;
+  } catch (const std::exception &e) {
+    std::fprintf(stderr, "%s\n", e.what());
+    return 1;
+  }
+}
+
+static std::vector<char> file_bytes(const std::string &path) {
+  std::vector<char> out;
+  FILE *f = std::fopen(path.c_str(), "rb");
+  if (!f) return out;
+  char buf[1 << 16];
+  size_t r;
+  while ((r = std::fread(buf, 1, sizeof buf, f)) > 0) out.insert(out.end(), buf, buf + r);
+  std::fclose(f);
+  return out;
+}
+
+// __cuda_resolve::rebuild (influence-matrix columns batched on the device)
+// against the reference's __resolve::rebuild, both over a __cuda on a
+// __vring(radius, core, layers).  Resolved strengths into batched / percol;
+// *same_file = 1 when the two .wakeinfluence files are byte-identical.
+int dropin_vring_resolve_batched(double radius, double core, int layers, double *batched,
+                                 double *percol, int *same_file) {
+  try {
+    pawan::__vring *Vb = new pawan::__vring(radius, core, layers);
+    pawan::__vring *Vp = new pawan::__vring(radius, core, layers);
+    ReadCuda *B = new ReadCuda(Vb, 0.0, PAWAN_PREC_F32, 0);
+    ReadCuda *P = new ReadCuda(Vp, 0.0, PAWAN_PREC_F32, 0);
+    pawan::__io io;
+    const std::string path = io.getFile() + ".wakeinfluence";
+    pawan::__cuda_resolve batched_resolve;
+    batched_resolve.rebuild(B, &io);
+    const std::vector<char> fb = file_bytes(path);
+    pawan::__resolve reference_resolve;
+    reference_resolve.rebuild(P, &io);
+    const std::vector<char> fp = file_bytes(path);
+    *same_file = (!fb.empty() && fb == fp) ? 1 : 0;
+    gsl_vector_view vb = gsl_vector_view_array(batched, B->_size);
+    gsl_vector_view vp = gsl_vector_view_array(percol, P->_size);
+    B->getStates(&vb.vector);
+    P->getStates(&vp.vector);
+    delete B;
+    delete P;
+    delete Vb;
+    delete Vp;
     return 0;
   } catch (const std::exception &e) {
     std::fprintf(stderr, "%s\n", e.what());

@@ -46,6 +46,40 @@ def test_influence_matches_oracle_mixed_radii_many_wakes(ctx):
     check(s.influence(), oracle.influence(pos, vor, rad))
 
 
+@pytest.mark.parametrize("kernel", ["highorder", "gaussian"])
+def test_influence_columns_bit_identical_to_single_column(ctx, kernel):
+    """Eleven strength columns (one full group of eight and a partial one) in
+    one call: each column equals the single-column field of that strength bit
+    for bit, matches the oracle, and the system's own strengths are untouched."""
+    sc = g.ring_pair(n_stations=40, seed=31, nu=0.0)  # N = 640, not a multiple of 128
+    pos, vor, rad, vol = sc.union()
+    rad = rad * np.random.default_rng(6).uniform(0.8, 1.2, rad.shape)
+    s = System(ctx, sc.counts, 0.0, "f32")
+    s.set_kernel(kernel)
+    s.set_particles(pos, vor, rad, vol)
+    own = s.influence()
+    cols = np.random.default_rng(7).standard_normal((11, sc.n, 3))
+    k = s.influence_columns(cols)
+    assert np.array_equal(s.influence(), own)
+    for c in range(cols.shape[0]):
+        s.set_particles(pos, cols[c], rad, vol)
+        assert np.array_equal(k[c], s.influence()), c
+        check(k[c], oracle.influence(pos, cols[c], rad, kernel=kernel))
+
+
+def test_influence_columns_rejects_bad_sizes(ctx):
+    sc = g.single_ring(n_stations=8, seed=1)
+    s = System.from_scenario(ctx, sc, "f32")
+    a = np.zeros((2, sc.n, 3))
+    k = np.empty_like(a)
+    f = s._lib.pawan_system_influence_columns
+    assert f(s.handle, 2, a.ctypes.data_as(_dp), k.ctypes.data_as(_dp), a.size - 3) == 1
+    assert f(s.handle, 0, a.ctypes.data_as(_dp), k.ctypes.data_as(_dp), 0) == 1
+    assert f(s.handle, 2, None, k.ctypes.data_as(_dp), a.size) == 1
+    with pytest.raises(ValueError):
+        s.influence_columns(np.zeros((2, sc.n + 1, 3)))
+
+
 def test_influence_follows_the_state(ctx):
     """After RK4 steps and after set_states the field is that of the new state."""
     sc = g.ring_pair(n_stations=64, seed=24, nu=1e-3)
@@ -72,6 +106,8 @@ def lib():
     L = ctypes.CDLL(LIB)
     L.dropin_influence.argtypes = [ctypes.c_int, _szp, _dp, _dp, _dp, _dp, _dp, _dp]
     L.dropin_vring_resolve.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _dp]
+    L.dropin_vring_resolve_batched.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp,
+                                               _dp, ctypes.POINTER(ctypes.c_int)]
     return L
 
 
@@ -108,3 +144,36 @@ def test_dropin_vring_resolve_matches_reference(lib):
     assert np.array_equal(cpu, d["strengths"])
     # an LU solve of a matrix whose entries agree to ~1e-15
     assert rms_rel(gpu, cpu) < 1e-10 and max_rel(gpu, cpu) < 1e-10
+
+
+def _in_data_dir(fn):
+    cwd = os.getcwd()
+    with tempfile.TemporaryDirectory() as tmp:
+        os.makedirs(os.path.join(tmp, "data"))
+        os.chdir(tmp)
+        try:
+            return fn()
+        finally:
+            os.chdir(cwd)
+
+
+@needs_lib
+@pytest.mark.parametrize("radius,core,layers", [(1.0, 0.1, 1), (1.0, 0.1, 2)])
+def test_dropin_batched_resolve_matches_reference_rebuild(lib, radius, core, layers):
+    """__cuda_resolve::rebuild (all (2L+1)^2 influence columns in one device
+    call) against the reference's __resolve::rebuild over the same __cuda (one
+    solve per column): the same resolved strengths bit for bit and a
+    byte-identical .wakeinfluence file.  layers = 2 is the vring the
+    reference's main() resolves (25 columns, 3,950 particles)."""
+    n = (2 * layers + 1) ** 2
+    b, p = np.empty(n), np.empty(n)
+    same = ctypes.c_int(0)
+    st = _in_data_dir(lambda: lib.dropin_vring_resolve_batched(
+        radius, core, layers, b.ctypes.data_as(_dp), p.ctypes.data_as(_dp), ctypes.byref(same)))
+    assert st == 0
+    assert same.value == 1
+    assert np.array_equal(b, p)
+    if layers == 1:
+        d = load("vring1_resolve")
+        assert float(d["radius"]) == radius and float(d["core"]) == core and int(d["layers"]) == 1
+        assert rms_rel(b, d["strengths"]) < 1e-10 and max_rel(b, d["strengths"]) < 1e-10
