@@ -73,6 +73,39 @@ def test_ragged_sizes_against_restatement(ctx, n):
         check(prec, *s.union_rates(), u_ref, da_ref)
 
 
+@pytest.mark.parametrize("prec", PRECS)
+def test_coincident_particles_give_nan_where_the_reference_does(ctx, prec):
+    """Distinct particles at one position: the reference's kernel is singular
+    at rho = 0 (q and F divide by rho, highorder.h:58-59), so in its solve
+    those particles' rates are NaN and every other particle's are finite.
+    The GPU paths exclude only the self pair, by index, as the reference does
+    (interaction.cpp:158-173): NaN in the same rows, the other rows within
+    tolerance.  One coincident pair shares a 128-tile, one spans two tiles."""
+    rng = np.random.default_rng(11)
+    n = 300
+    pos = rng.uniform(-1, 1, (n, 3))
+    pos[100] = pos[7]
+    pos[250] = pos[40]
+    vor = rng.normal(0, 0.01, (n, 3))
+    rad = rng.uniform(0.05, 0.2, n)
+    vol = rng.uniform(1e-4, 2e-4, n)
+    if oracle.ref_available():
+        r = oracle.RefSystem([n], pos, vor, rad, vol, 1e-3)
+        r.solve()
+        u_ref, da_ref = r.union_rates()
+    else:
+        u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, 1e-3)
+    bad = np.isnan(u_ref).any(axis=1) | np.isnan(da_ref).any(axis=1)
+    assert sorted(np.flatnonzero(bad)) == [7, 40, 100, 250]
+    s = System(ctx, [n], 1e-3, prec)
+    s.set_particles(pos, vor, rad, vol)
+    s.solve()
+    u, da = s.union_rates()
+    assert np.array_equal(np.isnan(u).all(axis=1) & np.isnan(da).all(axis=1), bad)
+    assert np.isfinite(u[~bad]).all() and np.isfinite(da[~bad]).all()
+    check(prec, u[~bad], da[~bad], u_ref[~bad], da_ref[~bad])
+
+
 def test_many_wakes_union(ctx):
     """Five wakes of uneven size: all pairs over the union, like interact()."""
     rng = np.random.default_rng(5)
@@ -214,6 +247,8 @@ def test_invalid_arguments_raise(ctx):
     with pytest.raises(pawan_b200.PawanError):
         System(ctx, [1], 0.0)  # a single particle interacts with nothing
     with pytest.raises(pawan_b200.PawanError):
+        System(ctx, [5, 0, 7], 0.0)  # an empty wake (the reference's GSL aborts on it)
+    with pytest.raises(pawan_b200.PawanError):
         System(ctx, [10], -1.0)
     s = System(ctx, [10], 0.0)
     with pytest.raises(pawan_b200.PawanError):
@@ -239,8 +274,9 @@ def test_full_size_sampled_targets(ctx, name):
     assert np.abs(da_all.sum(axis=0)).max() < 1e-5 * np.abs(da_all).sum()
 
 
+@pytest.mark.parametrize("mixed", [False, True])
 @pytest.mark.parametrize("gap", [3.0, 4.5, 5.5, 6.5, 10.0])
-def test_tile_classes_at_their_boundaries(ctx, gap):
+def test_tile_classes_at_their_boundaries(ctx, gap, mixed):
     """Two compact clusters of 256 particles (two 128-tiles each) whose boxes
     are `gap` smoothing radii apart: near (< 4 s), far with the Z terms
     (4 s .. 6 s) and far without them (>= 6 s, where Z is below 3e-9 of q).
@@ -249,7 +285,9 @@ def test_tile_classes_at_their_boundaries(ctx, gap):
     B's strengths doubled, minus the first solve, is at A exactly the part of
     A's rates that B's strengths drive (A's own tiles compute identically in
     both solves), compared with the same difference in the oracle.  nu != 0;
-    packed and scalar tilings."""
+    packed and scalar tilings; one smoothing radius (the uniform-radius
+    forms) or radii in [0.8 s, 1.2 s] (the general forms; the Z-free class
+    then starts at 7.2 s)."""
     rng = np.random.default_rng(int(gap * 10))
     s = 0.05
     n = 256
@@ -260,7 +298,7 @@ def test_tile_classes_at_their_boundaries(ctx, gap):
     vor = rng.normal(size=(2 * n, 3)) * 1e-3
     vor2 = vor.copy()
     vor2[n:] *= 2.0
-    rad = np.full(2 * n, s)
+    rad = s * rng.uniform(0.8, 1.2, 2 * n) if mixed else np.full(2 * n, s)
     vol = np.full(2 * n, 1e-5)
     nu = 1e-3
     u1, da1 = oracle.pairs(pos, vor, rad, vol, nu)
