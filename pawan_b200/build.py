@@ -35,7 +35,7 @@ PER_FILE = {
     "pair_plain.cu": ["--fmad=false"],
 }
 SOURCES = ["pair_f32.cu", "pair_f64.cu", "pair_plain.cu", "stage.cu", "diag.cu", "influence.cu",
-           "peak.cu", "runtime.cpp", "serve.cpp", "writer.cpp", "noalloc.cu"]
+           "peak.cu", "runtime.cpp", "abi.cpp", "serve.cpp", "writer.cpp", "noalloc.cu"]
 
 
 def nvcc() -> str:

@@ -183,6 +183,27 @@ struct Plan {
 int fail(pawan_ctx *ctx, int code, const std::string &msg);
 int cuda_fail(pawan_ctx *ctx, cudaError_t e, const char *where);
 
+// Return the status of a failed CUDA call (recorded on ctx) or of a failed
+// library call, from the enclosing function.
+#define PAWAN_CUDA(ctx, expr)                                           \
+  do {                                                                  \
+    cudaError_t e_ = (expr);                                            \
+    if (e_ != cudaSuccess) return ::pawan::cuda_fail((ctx), e_, #expr); \
+  } while (0)
+
+#define PAWAN_TRY(expr)            \
+  do {                             \
+    int s_ = (expr);               \
+    if (s_ != PAWAN_OK) return s_; \
+  } while (0)
+
+// Process blocks of a sharded system start at multiples of kShardAlign
+// particles: whole stage blocks and whole target tiles of every tiling.
+constexpr size_t kShardAlign = 512;
+
+// Whether a precision's kernels are compiled for a tiling and smoothing kernel.
+bool tile_supported(int precision, const PairConfig &pc, int kernel);
+
 int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int precision,
                const TileChoice &tile, std::unique_ptr<Plan> &out, int fixed_chunk_sources = 0,
                bool ordered_alloc = false);

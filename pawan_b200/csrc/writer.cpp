@@ -24,12 +24,6 @@
 
 using namespace pawan;
 
-#define PAWAN_TRY(expr)            \
-  do {                             \
-    int s_ = (expr);               \
-    if (s_ != PAWAN_OK) return s_; \
-  } while (0)
-
 // The writer's CUDA calls report through the context like the rest of the ABI.
 #define PAWAN_CUDA_RET(expr)                                  \
   do {                                                        \
