@@ -67,6 +67,27 @@ def test_influence_columns_bit_identical_to_single_column(ctx, kernel):
         check(k[c], oracle.influence(pos, cols[c], rad, kernel=kernel))
 
 
+def test_influence_columns_split_over_launches(ctx):
+    """More columns than the 256 MiB device scratch holds (1,365 columns of
+    N = 4,096): the columns run in two launches, and the columns on either
+    side of the split, and the last, equal single-column solves."""
+    rng = np.random.default_rng(8)
+    n = 4096
+    pos = rng.uniform(-1, 1, (n, 3))
+    rad = rng.uniform(0.05, 0.1, n)
+    vol = np.full(n, 1e-4)
+    ncols = 1400
+    fit = (256 << 20) // (2 * 3 * n * 8)
+    assert fit < ncols
+    cols = rng.standard_normal((ncols, n, 3))
+    s = System(ctx, [n], 0.0, "f32")
+    s.set_particles(pos, cols[0], rad, vol)
+    k = s.influence_columns(cols)
+    for c in (0, fit - 1, fit, ncols - 1):
+        s.set_particles(pos, cols[c], rad, vol)
+        assert np.array_equal(k[c], s.influence()), c
+
+
 def test_influence_columns_rejects_bad_sizes(ctx):
     sc = g.single_ring(n_stations=8, seed=1)
     s = System.from_scenario(ctx, sc, "f32")
