@@ -254,6 +254,11 @@ def cpu_reference_sample(pos, vor, rad, vol, nu, target_s: float, cap_n: int = 1
         n = min(cap_n, int(n * grow) // 8 * 8)
 
 
+def workload_name(sc) -> str:
+    """The workload both arms of the bench report in config.workload."""
+    return f"leapfrogging coaxial ring pair, N={sc.n}, nu={sc.nu}, dt={sc.dt}, RK4 step"
+
+
 def run_reference(args, rk: Ranks):
     from pawan_b200 import geometry as g
     if rk.rank != 0:
@@ -282,8 +287,9 @@ def run_reference(args, rk: Ranks):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded ring pair geometry)",
-            "config": {"workload": f"ring_pair N={sc.n} (sampled to {n} particles on CPU)",
-                       "n_particles": sc.n, "sample_particles": n, "nu": sc.nu},
+            "config": {"workload": workload_name(sc), "n_particles": sc.n, "wakes": len(sc.counts),
+                       "precision": "fp64 (the reference's)", "parallelism": f"host threads x{threads}",
+                       "sample_particles": n},
             "cpu_baseline": {"value": value, "unit": "G interactions/s", "cores": threads,
                              "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": "G interactions/s", "h2d_bytes_per_step": 0,
@@ -470,7 +476,7 @@ def run_pawan(args, rk: Ranks):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded ring pair geometry, jitter 1e-4)",
-            "config": {"workload": f"leapfrogging coaxial ring pair, N={N}, nu={sc.nu}, dt={dt}, RK4 step",
+            "config": {"workload": workload_name(sc),
                        "n_particles": N, "wakes": len(sc.counts), "precision": "fp32 pairs, fp64 accumulation+state",
                        "parallelism": f"replicas x{rk.world}", "l2": "flushed between timed steps (256 MiB write)",
                        "state": "restored to the initial geometry before every step (device copy)",
@@ -609,7 +615,7 @@ def run_strong(args, rk: Ranks):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded ring pair geometry, jitter 1e-4)",
-            "config": {"workload": f"leapfrogging coaxial ring pair, N={N}, nu={sc.nu}, dt={dt}, RK4 step",
+            "config": {"workload": workload_name(sc),
                        "n_particles": N, "precision": "fp32 pairs, fp64 accumulation+state",
                        "parallelism": f"target shards x{rk.world} (NCCL all-gather of 48 B/particle per RK4 stage)",
                        "shard_particles": sh.size, "allgather_bytes_per_step": 4 * 8 * 6 * sh.size * rk.world,
