@@ -228,9 +228,28 @@ def state_update_roofline(prof_stage: dict) -> dict:
                     "partly L2-resident, so frac can exceed 1"}
 
 
-def traffic_from_profiles():
-    """DRAM bytes per pair launch from the committed ncu summary, if any."""
-    return profile_summary().get("dram_bytes_per_launch_full_size")
+def profiled_tiling_matches(tile: dict) -> bool:
+    """Whether the committed ncu summary was captured with this tiling (its
+    traffic and pipe figures depend on it: chunking sets the partial-sum bytes)."""
+    prof = profile_summary().get("tile")
+    return bool(prof) and all(tile.get(k) == v for k, v in prof.items())
+
+
+def traffic_from_profiles(tile: dict):
+    """DRAM bytes per pair launch from the committed ncu summary, when it was
+    captured with the timed tiling; else None."""
+    return profile_summary().get("dram_bytes_per_launch_full_size") if profiled_tiling_matches(tile) else None
+
+
+def executed_from_profiles(tile: dict) -> dict:
+    """Executed-work figures of the committed ncu summary and the tiling they
+    were measured with (the same as the timed one or not, as `same_tiling` says)."""
+    prof = profile_summary()
+    out = {k: prof.get(k) for k in ("fma_pipe_active", "fma_pipe_lane_ops_per_interaction",
+                                    "thread_instructions_per_interaction")}
+    out["profiled_kernel"] = prof.get("kernel")
+    out["same_tiling"] = profiled_tiling_matches(tile)
+    return out
 
 
 # ------------------------------------------------------------ CPU baseline
@@ -484,7 +503,7 @@ def run_pawan(args, rk: Ranks):
             "gpu_launches": int(launches), "clocks": clk,
             "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": peak_tflops,
                          "unit": "TFLOP/s", "frac": achieved_tflops / peak_tflops,
-                         "traffic": traffic_from_profiles(),
+                         "traffic": traffic_from_profiles(tuned),
                          "kernel": "pairs_f32_kernel", "flops_per_interaction": flops,
                          "pair_launch_ms": pair_avg_s * 1e3,
                          "peak_source": "measured: FFMA-chain probe (pawan_peak_fp32) in this run",
@@ -492,9 +511,7 @@ def run_pawan(args, rk: Ranks):
                                  "kernel executes fewer (per-tile crosses; Z terms formed only where they "
                                  "are above FP32 resolution), so frac can exceed 1. Executed-work "
                                  "utilisation: ncu FMA-pipe activity in executed_ncu",
-                         "executed_ncu": {k: profile_summary().get(k) for k in
-                                          ("fma_pipe_active", "fma_pipe_lane_ops_per_interaction",
-                                           "thread_instructions_per_interaction")}},
+                         "executed_ncu": executed_from_profiles(tuned)},
             "state_update": state_update_roofline(prof_stage)}
 
     if not args.quick:
