@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import oracle
-from pawan_b200 import Batch, System, union_to_state
+from pawan_b200 import Batch, PawanError, System, union_to_state
 from pawan_b200 import geometry as g
 from helpers import TOL_F32_RMS, rms_rel
 
@@ -44,6 +44,36 @@ def test_batch_rk4_matches_solo_and_restatement(ctx, use_graph):
         p, v = oracle.rk4_step(pos, vor, rad, vol, sc.nu, dts[k], 3)
         ref = union_to_state(sc.counts, p, v)
         assert rms_rel(a - st0, ref - st0) <= TOL_F32_RMS
+
+
+def test_gaussian_batch_matches_solo_and_restatement(ctx):
+    """Systems with the reference's Gaussian smoothing kernel batched in one
+    launch per stage: the same steps as each system alone, and the FP64
+    restatement's with that kernel within the FP32 tolerance."""
+    scs = small_batch(seed=7)
+    systems = [System.from_scenario(ctx, sc, "f32") for sc in scs]
+    solos = [System.from_scenario(ctx, sc, "f32") for sc in scs]
+    for s in systems + solos:
+        s.set_kernel("gaussian")
+    b = Batch(ctx, systems)
+    b.rk4(scs[0].dt, 2)
+    for sc, s, solo in zip(scs, systems, solos):
+        solo.rk4(scs[0].dt, 2)
+        st0 = sc.state()
+        a, c = s.get_states(), solo.get_states()
+        assert rms_rel(a - st0, c - st0) < 1e-12
+        pos, vor, rad, vol = sc.union()
+        p, v = oracle.rk4_step(pos, vor, rad, vol, sc.nu, scs[0].dt, 2, kernel="gaussian")
+        ref = union_to_state(sc.counts, p, v)
+        assert rms_rel(a - st0, ref - st0) <= TOL_F32_RMS
+
+
+def test_batch_rejects_mixed_smoothing_kernels(ctx):
+    scs = small_batch(n_solves=2, seed=8)
+    systems = [System.from_scenario(ctx, sc, "f32") for sc in scs]
+    systems[1].set_kernel("gaussian")
+    with pytest.raises(PawanError):
+        Batch(ctx, systems)
 
 
 def test_graph_and_eager_agree_bitwise(ctx):
