@@ -188,7 +188,11 @@ int pawan_system_integrate(pawan_system *sys, double T, size_t n, const char *pa
 int pawan_system_integrate_file(pawan_system *sys, double T, size_t n, void *file, int method);
 int pawan_system_set_tiling(pawan_system *sys, const pawan_tiling *tiling);
 int pawan_system_get_tiling(pawan_system *sys, pawan_tiling *tiling);
-/* Times every compiled tiling on this system and keeps the fastest. */
+/* Times the candidate tilings and chunkings on this system -- each one
+ * right-hand side as an RK4 stage runs it: the pair launch and the reduction
+ * of its chunk partials -- and keeps the fastest.  The state is unchanged; the
+ * last rates (pawan_system_get_rates) are left as those of the current state,
+ * computed with one of the candidates. */
 int pawan_system_autotune(pawan_system *sys);
 /* Device-side snapshot of the state (checkpoint) and its restore, for
  * resuming a run or repeating steps from one state.  The reference's
@@ -241,6 +245,7 @@ int pawan_batch_rk4(pawan_batch *batch, const double *dt, double dt0, size_t nst
                     int use_graph);
 int pawan_batch_solve(pawan_batch *batch);
 int pawan_batch_set_tiling(pawan_batch *batch, const pawan_tiling *tiling);
+/* The same over the batch's systems together. */
 int pawan_batch_autotune(pawan_batch *batch);
 
 /* ---------------------------------------------------------------- serving */

@@ -483,13 +483,20 @@ int autotune_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, in
   double best_ms = 1e300;
   TileChoice best_t = default_tile(precision);
   int status = PAWAN_OK;
+  // One right-hand side as an RK4 stage runs it: the pair launch and the
+  // reduction of its chunk partials (STAGE_RATES writes only the rates
+  // buffer), so that finer chunking pays for the partials it adds.
+  auto rhs = [&](Plan &p) -> int {
+    PAWAN_TRY(launch_pairs(ctx, p, false));
+    return launch_stage_mode(ctx, p, STAGE_RATES);
+  };
   auto time_tile = [&](const TileChoice &t, double *ms) -> int {
     std::unique_ptr<Plan> p;
     PAWAN_TRY(build_plan(ctx, systems, precision, t, p));
-    PAWAN_TRY(launch_pairs(ctx, *p, false));  // warm-up
+    PAWAN_TRY(rhs(*p));  // warm-up
     PAWAN_CUDA(ctx, cudaEventRecord(e0, ctx->stream));
     const int reps = 2;
-    for (int r = 0; r < reps; ++r) PAWAN_TRY(launch_pairs(ctx, *p, false));
+    for (int r = 0; r < reps; ++r) PAWAN_TRY(rhs(*p));
     PAWAN_CUDA(ctx, cudaEventRecord(e1, ctx->stream));
     PAWAN_CUDA(ctx, cudaEventSynchronize(e1));
     float f = 0.f;
