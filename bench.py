@@ -256,11 +256,13 @@ def executed_from_profiles(tile: dict) -> dict:
 
 def cpu_reference_sample(pos, vor, rad, vol, nu, target_s: float, cap_n: int = 16384):
     """Times the reference's OpenMP __parallel::solve() on the first n particles
-    of the workload, growing n until one solve takes about target_s seconds.
+    of the workload, growing n until one solve takes about target_s seconds
+    (at most cap_n and the workload's own size).
     Returns (interactions per second, n, seconds, threads)."""
     import oracle
     threads = oracle.ref_max_threads()
-    n = 1024
+    cap_n = min(cap_n, len(rad))
+    n = min(1024, cap_n)
     while True:
         ref = oracle.RefSystem([n], pos[:n], vor[:n], rad[:n], vol[:n], nu, parallel=True)
         t0 = oracle.ref_wtime()

@@ -1,8 +1,11 @@
 """Multi-rank host logic of bench.py over gloo on CPU (world size 2): rank
 discovery from the torchrun environment, barriers, the max-over-ranks timing
-reduction and the whole-job aggregation."""
+reduction and the whole-job aggregation, and the reference arm under torchrun
+(rank 0 alone runs and prints; the other ranks exit 0 without work)."""
+import json
 import os
 import socket
+import subprocess
 import sys
 
 import pytest
@@ -61,3 +64,22 @@ def test_single_rank_needs_no_process_group():
     rk = bench.Ranks(1)
     assert rk.world == 1 and rk.dist is None and rk.max(3.5) == 3.5
     rk.close()
+
+
+def test_reference_arm_under_two_ranks():
+    sys.path.insert(0, ROOT)
+    import oracle
+    if not oracle.ref_available():
+        pytest.skip("the reference's sources are not compiled here (make -C oracle)")
+    env = dict(os.environ, PAWAN_BENCH_BACKEND="gloo", OMP_NUM_THREADS="2")
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
+           "--master-addr", "127.0.0.1", "--master-port", str(_free_port()),
+           os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1",
+           "--warmup", "1", "--n-stations", "128"]
+    r = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, r.stdout
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "reference" and d["config"]["n_particles"] == 2048
