@@ -129,6 +129,10 @@ int pawan_system_get_wake_rates(pawan_system *sys, size_t wake, double *velocity
 /* nsteps of __rk4::step (src/integration/rk4.cpp:12-76), state kept on the
  * device between steps; read it back with get_states. */
 int pawan_system_rk4(pawan_system *sys, double dt, size_t nsteps);
+/* The same with the step's four (pair, stage) launch pairs captured once in a
+ * CUDA graph and replayed per step (bit-identical to pawan_system_rk4; the
+ * pair launches are not timed by pawan_ctx_profile). */
+int pawan_system_rk4_graph(pawan_system *sys, double dt, size_t nsteps);
 /* nsteps of __integration::step (src/integration/integration.cpp:37-45). */
 int pawan_system_euler(pawan_system *sys, double dt, size_t nsteps);
 /* __interaction::diagnose (interaction.cpp:49-93), FP64 on the device.
@@ -194,6 +198,13 @@ int pawan_system_get_tiling(pawan_system *sys, pawan_tiling *tiling);
  * last rates (pawan_system_get_rates) are left as those of the current state,
  * computed with one of the candidates. */
 int pawan_system_autotune(pawan_system *sys);
+/* The tilings pawan_system_autotune / pawan_batch_autotune time for a
+ * precision and smoothing kernel (each at the default chunking): *count is
+ * their number, the first min(cap, *count) are written to out.  The
+ * autotuner then times the chunkings pawan_tile_chunkings lists
+ * (items_per_slot) for the fastest.  Host-only; no device needed. */
+int pawan_tile_candidates(int precision, int kernel, pawan_tiling *out, size_t cap, size_t *count);
+int pawan_tile_chunkings(int *out, size_t cap, size_t *count);
 /* Device-side snapshot of the state (checkpoint) and its restore, for
  * resuming a run or repeating steps from one state.  The reference's
  * file-based save()/read() (src/wake/wake.cpp:58-85) is the on-disk
@@ -323,19 +334,23 @@ int pawan_server_inject(pawan_server *srv, int fault, int count, double seconds)
 
 /* ------------------------------------------------- allocation-free solve */
 /* No counterpart in the reference.  For callers that must not allocate device
- * memory -- inside someone else's stream capture or host callback, under an
- * allocator that owns the whole device, or in a latency-critical loop where
- * cudaMalloc's implicit synchronisation is not acceptable.  One FP32 solve
- * (all pairs over the n particles, as pawan_system_solve with
- * PAWAN_PREC_F32) from caller-owned DEVICE arrays: position and vorticity
- * n x 3, radius and volume n; writes velocity and vorticity rate (n x 3,
- * device).  All working memory is one static device array reserved by every
- * GPU that loads the library (about 4.2 MB), so n <= PAWAN_NOALLOC_MAX_PARTICLES;
- * larger n returns PAWAN_ERR_INVALID.  The first call on a device resolves that
- * array's address (make it before any stream capture).  Calls share the
- * array: calls that may overlap on the GPU must be serialised by the caller.
- * `stream` is a cudaStream_t (NULL: the default stream); the call is
- * asynchronous on it and allocates nothing. */
+ * memory -- inside a host callback, under an allocator that owns the whole
+ * device, or in a latency-critical loop where cudaMalloc's implicit
+ * synchronisation is not acceptable.  One FP32 solve (all pairs over the n
+ * particles with the high-order smoothing kernel, whatever
+ * pawan_system_set_kernel chose elsewhere) from caller-owned DEVICE arrays:
+ * position and vorticity n x 3, radius and volume n; writes velocity and
+ * vorticity rate (n x 3, device).  The pair kernel is pawan_system_solve's
+ * with PAWAN_PREC_F32, but the FP32 positions are relative to particle 0
+ * rather than the centroid, so results agree with pawan_system_solve within
+ * the FP32 tolerance, not bit for bit.  All working memory is one static
+ * device array reserved by every GPU that loads the library (about 4.2 MB),
+ * so n <= PAWAN_NOALLOC_MAX_PARTICLES; larger n, n < 2 or a negative or
+ * non-finite nu returns PAWAN_ERR_INVALID.  The first call on a device
+ * resolves that array's address (make it before any stream capture).  Calls
+ * share the array: calls that may overlap on the GPU race and must be
+ * serialised by the caller.  `stream` is a cudaStream_t (NULL: the default
+ * stream); the call is asynchronous on it and allocates nothing. */
 #define PAWAN_NOALLOC_MAX_PARTICLES 16384
 int pawan_interact_noalloc(const double *position, const double *vorticity, const double *radius,
                            const double *volume, size_t n, double nu, double *velocity,

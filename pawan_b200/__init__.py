@@ -109,6 +109,7 @@ _SIGS = {
     "pawan_system_get_rates": (ctypes.c_int, [_vp, _dp, ctypes.c_size_t]),
     "pawan_system_get_wake_rates": (ctypes.c_int, [_vp, ctypes.c_size_t, _dp, _dp]),
     "pawan_system_rk4": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_size_t]),
+    "pawan_system_rk4_graph": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_size_t]),
     "pawan_system_euler": (ctypes.c_int, [_vp, ctypes.c_double, ctypes.c_size_t]),
     "pawan_system_diagnose": (ctypes.c_int, [_vp, _dp, ctypes.c_int]),
     "pawan_system_kinetic_energy": (ctypes.c_int, [_vp, _dp]),
@@ -132,6 +133,9 @@ _SIGS = {
     "pawan_system_set_tiling": (ctypes.c_int, [_vp, ctypes.POINTER(Tiling)]),
     "pawan_system_get_tiling": (ctypes.c_int, [_vp, ctypes.POINTER(Tiling)]),
     "pawan_system_autotune": (ctypes.c_int, [_vp]),
+    "pawan_tile_candidates": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(Tiling), ctypes.c_size_t,
+                                             _szp]),
+    "pawan_tile_chunkings": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.c_size_t, _szp]),
     "pawan_system_device_state": (ctypes.c_int, [_vp, ctypes.POINTER(_dp)]),
     "pawan_system_checkpoint": (ctypes.c_int, [_vp]),
     "pawan_system_restore": (ctypes.c_int, [_vp]),
@@ -376,8 +380,11 @@ class System:
         us, das = zip(*(self.wake_rates(w) for w in range(len(self.counts))))
         return np.concatenate(us), np.concatenate(das)
 
-    def rk4(self, dt: float, nsteps: int = 1):
-        self.ctx.check(self._lib.pawan_system_rk4(self._h, float(dt), int(nsteps)))
+    def rk4(self, dt: float, nsteps: int = 1, use_graph: bool = False):
+        """nsteps of __rk4::step on the device; use_graph replays the step's
+        launches from a CUDA graph (same bits)."""
+        fn = self._lib.pawan_system_rk4_graph if use_graph else self._lib.pawan_system_rk4
+        self.ctx.check(fn(self._h, float(dt), int(nsteps)))
 
     def euler(self, dt: float, nsteps: int = 1):
         self.ctx.check(self._lib.pawan_system_euler(self._h, float(dt), int(nsteps)))
@@ -622,6 +629,52 @@ def interact_noalloc(position: int, vorticity: int, radius: int, volume: int, n:
     lib = load_library()
     return int(lib.pawan_interact_noalloc(position, vorticity, radius, volume, int(n), float(nu),
                                           velocity, retvorcity, stream or None))
+
+
+def tile_candidates(precision: str = "f32", kernel: str = "highorder") -> list:
+    """The tilings the autotuner times (dicts as System.get_config returns);
+    host-only, no GPU needed."""
+    lib = load_library()
+    n = ctypes.c_size_t(0)
+    st = lib.pawan_tile_candidates(PREC[precision], KERNELS[kernel], None, 0, ctypes.byref(n))
+    if st != OK:
+        raise PawanError(st, "tile_candidates")
+    arr = (Tiling * max(1, n.value))()
+    lib.pawan_tile_candidates(PREC[precision], KERNELS[kernel], arr, n.value, ctypes.byref(n))
+    return [{f: getattr(arr[i], f) for f, _ in Tiling._fields_} for i in range(n.value)]
+
+
+def tile_chunkings() -> list:
+    """The chunkings (work items per resident block) the autotuner times."""
+    lib = load_library()
+    n = ctypes.c_size_t(0)
+    lib.pawan_tile_chunkings(None, 0, ctypes.byref(n))
+    arr = (ctypes.c_int * max(1, n.value))()
+    lib.pawan_tile_chunkings(arr, n.value, ctypes.byref(n))
+    return list(arr[:n.value])
+
+
+def rms_rel(a, b) -> float:
+    """||a - b||_2 / ||b||_2 over all components: the RMS relative error the
+    tests and the bench state against a reference b."""
+    a, b = np.asarray(a, dtype=np.float64).ravel(), np.asarray(b, dtype=np.float64).ravel()
+    den = np.linalg.norm(b)
+    return float(np.linalg.norm(a - b) / den) if den > 0 else float(np.linalg.norm(a - b))
+
+
+def max_rel(a, b) -> float:
+    """max |a - b| / max |b|: the largest error relative to the largest
+    reference value (per-component relative error is ill-conditioned where
+    the reference is near 0)."""
+    a, b = np.asarray(a, dtype=np.float64).ravel(), np.asarray(b, dtype=np.float64).ravel()
+    den = np.abs(b).max()
+    return float(np.abs(a - b).max() / den) if den > 0 else float(np.abs(a - b).max())
+
+
+def error_stats(u, da, u_ref, da_ref) -> dict:
+    """RMS and max relative error of velocity and vorticity rate."""
+    return {"u_rms_rel": rms_rel(u, u_ref), "u_max_rel": max_rel(u, u_ref),
+            "dalpha_rms_rel": rms_rel(da, da_ref), "dalpha_max_rel": max_rel(da, da_ref)}
 
 
 def union_to_state(counts: Sequence[int], pos: np.ndarray, vor: np.ndarray) -> np.ndarray:

@@ -381,6 +381,14 @@ int pawan_system_rk4(pawan_system *sys, double dt, size_t nsteps) {
   return rk4_steps(sys->ctx, *sys->plan, nsteps, false);
 }
 
+int pawan_system_rk4_graph(pawan_system *sys, double dt, size_t nsteps) {
+  CHECK_SYS(sys);
+  CHECK_UNSHARDED(sys);
+  PAWAN_TRY(system_ensure_plan(sys));
+  PAWAN_TRY(set_plan_dt(sys->ctx, *sys->plan, nullptr, dt));
+  return rk4_steps(sys->ctx, *sys->plan, nsteps, true);
+}
+
 int pawan_system_euler(pawan_system *sys, double dt, size_t nsteps) {
   CHECK_SYS(sys);
   CHECK_UNSHARDED(sys);
@@ -655,6 +663,31 @@ int pawan_system_get_tiling(pawan_system *sys, pawan_tiling *tiling) {
   tiling->blocks_per_sm = sys->tile.pc.minb;
   tiling->packed = sys->tile.pc.packed;
   tiling->items_per_slot = sys->tile.items_per_slot;
+  return PAWAN_OK;
+}
+
+int pawan_tile_candidates(int precision, int kernel, pawan_tiling *out, size_t cap, size_t *count) {
+  if (!count || (cap > 0 && !out)) return PAWAN_ERR_INVALID;
+  if (precision < PAWAN_PREC_F32 || precision > PAWAN_PREC_F64_PLAIN) return PAWAN_ERR_INVALID;
+  if (kernel != PAWAN_KERNEL_HIGHORDER && kernel != PAWAN_KERNEL_GAUSSIAN) return PAWAN_ERR_INVALID;
+  const std::vector<TileChoice> v = tile_candidates(precision, kernel);
+  *count = v.size();
+  for (size_t i = 0; i < v.size() && i < cap; ++i) {
+    out[i].threads = v[i].pc.tb;
+    out[i].threads_per_target = v[i].pc.p;
+    out[i].targets_per_thread = v[i].pc.r;
+    out[i].unroll = v[i].pc.unroll;
+    out[i].blocks_per_sm = v[i].pc.minb;
+    out[i].packed = v[i].pc.packed;
+    out[i].items_per_slot = v[i].items_per_slot;
+  }
+  return PAWAN_OK;
+}
+
+int pawan_tile_chunkings(int *out, size_t cap, size_t *count) {
+  if (!count || (cap > 0 && !out)) return PAWAN_ERR_INVALID;
+  *count = kTuneItemsPerSlot.size();
+  for (size_t i = 0; i < kTuneItemsPerSlot.size() && i < cap; ++i) out[i] = kTuneItemsPerSlot[i];
   return PAWAN_OK;
 }
 

@@ -515,7 +515,7 @@ int autotune_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, in
     }
   }
   if (status == PAWAN_OK) {
-    for (int ips : {4, 8, 32, 64, 128}) {
+    for (int ips : kTuneItemsPerSlot) {
       TileChoice t = best_t;
       t.items_per_slot = ips;
       double ms = 0;

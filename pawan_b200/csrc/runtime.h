@@ -73,7 +73,10 @@ struct TileChoice {
 };
 
 TileChoice default_tile(int precision);
+// Tilings the autotuner times (at the default chunking), and the chunkings
+// (work items per resident block) it then times for the fastest of them.
 std::vector<TileChoice> tile_candidates(int precision, int kernel);
+const std::vector<int> kTuneItemsPerSlot = {4, 8, 32, 64, 128};
 
 struct Plan;
 

@@ -54,3 +54,20 @@ def test_context_without_gpu_raises():
         pytest.skip("a GPU is present")
     with pytest.raises(pawan_b200.PawanError):
         pawan_b200.Context(0)
+
+
+def test_tile_candidates_listed_host_side():
+    """The autotuner's candidate tilings and chunkings, without a GPU; the
+    full-size parity tests (tests/test_gpu_pairs.py) run exactly these."""
+    from test_gpu_pairs import DEFAULT_TILING, TIMED_TILING, TUNE_CANDIDATES
+    keys = ("threads", "threads_per_target", "targets_per_thread", "unroll", "blocks_per_sm", "packed")
+    got = [tuple(c[k] for k in keys) for c in pawan_b200.tile_candidates("f32")]
+    assert got == TUNE_CANDIDATES
+    assert TIMED_TILING in got and DEFAULT_TILING in got
+    assert pawan_b200.tile_chunkings() == [4, 8, 32, 64, 128]
+    assert len(pawan_b200.tile_candidates("f64")) == 2
+    assert len(pawan_b200.tile_candidates("f32", "gaussian")) >= 2
+    lib = load_library()
+    n = ctypes.c_size_t(0)
+    assert lib.pawan_tile_candidates(9, 0, None, 0, ctypes.byref(n)) == 1
+    assert lib.pawan_tile_candidates(0, 0, None, 0, None) == 1

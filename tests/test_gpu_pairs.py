@@ -257,21 +257,68 @@ def test_invalid_arguments_raise(ctx):
         s.set_config(96, 1, 2, 16)
 
 
-@pytest.mark.parametrize("name", ["ring_pair", "helical_wake"])
-def test_full_size_sampled_targets(ctx, name):
-    """N = 131,072 (ring pair) and 262,144 (helical wake) in FP32: sampled
-    targets against the FP64 restatement summing over all N sources."""
-    sc = g.ring_pair(steps=1) if name == "ring_pair" else g.helical_wake(steps=1)
-    pos, vor, rad, vol = sc.union()
-    s = System.from_scenario(ctx, sc, "f32")
+# The tilings the autotuner times (pawan_tile_candidates; tests/test_abi.py
+# checks this list against the library's): (threads, threads per target,
+# targets per thread, unroll, blocks per SM, packed mode).
+TUNE_CANDIDATES = [(tb,) + sh for tb in (128, 256) for sh in (
+    (1, 1, 4, 0, 0), (2, 1, 4, 0, 0), (4, 1, 4, 0, 0), (1, 2, 1, 0, 0), (1, 2, 2, 0, 0),
+    (1, 1, 4, 5, 0), (1, 1, 1, 0, 1), (1, 1, 2, 0, 1), (1, 1, 4, 0, 1), (1, 1, 2, 5, 1),
+    (1, 1, 2, 0, 2), (1, 1, 4, 0, 2))
+    if not (tb == 256 and sh in ((1, 1, 4, 5, 0), (1, 1, 1, 0, 1), (1, 1, 2, 5, 1)))]
+# the tiling the default bench run's autotuner picks on the ring pair, and the
+# library's default tiling
+TIMED_TILING = (256, 1, 1, 4, 0, 1)
+DEFAULT_TILING = (128, 1, 1, 4, 0, 2)
+FULL_SAMPLES = 4096
+
+
+@pytest.fixture(scope="module")
+def full(ctx):
+    """Per workload, made on first use: (system, sampled targets, oracle rates
+    at them), the oracle summing 4,096 targets over all N sources in FP64."""
+    made = {}
+
+    def get(name):
+        if name not in made:
+            sc = g.ring_pair(steps=1) if name == "ring_pair" else g.helical_wake(steps=1)
+            pos, vor, rad, vol = sc.union()
+            t = np.sort(np.random.default_rng(0).choice(sc.n, FULL_SAMPLES, replace=False))
+            made[name] = (System.from_scenario(ctx, sc, "f32"), t,
+                          oracle.pairs(pos, vor, rad, vol, sc.nu, targets=t))
+        return made[name]
+    yield get
+    for s, _, _ in made.values():
+        s.close()
+
+
+def _check_full(full, name, tiling, ips):
+    s, t, (u_ref, da_ref) = full(name)
+    tb, p, r, unroll, minb, mode = tiling
+    s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=mode)
     s.solve()
     u, da = s.union_rates()
-    rng = np.random.default_rng(0)
-    t = np.sort(rng.choice(sc.n, 512, replace=False))
-    u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, sc.nu, targets=t)
     check("f32", u[t], da[t], u_ref, da_ref)
-    _, da_all = u, da
-    assert np.abs(da_all.sum(axis=0)).max() < 1e-5 * np.abs(da_all).sum()
+    assert np.abs(da.sum(axis=0)).max() < 1e-5 * np.abs(da).sum()
+
+
+@pytest.mark.parametrize("tiling", TUNE_CANDIDATES, ids=lambda c: "tiling" + "-".join(map(str, c)))
+@pytest.mark.parametrize("name", ["ring_pair", "helical_wake"])
+def test_full_size_every_candidate_tiling(full, name, tiling):
+    """N = 131,072 (ring pair) and 262,144 (helical wake) in FP32 with every
+    tiling the autotuner can pick, at its finest chunking (128 work items per
+    resident block): 4,096 sampled targets against the FP64 restatement
+    summed over all N sources."""
+    _check_full(full, name, tiling, 128)
+
+
+@pytest.mark.parametrize("ips", [4, 8, 16, 32, 64])
+@pytest.mark.parametrize("tiling", [TIMED_TILING, DEFAULT_TILING], ids=["timed", "default"])
+@pytest.mark.parametrize("name", ["ring_pair", "helical_wake"])
+def test_full_size_timed_tiling_every_chunking(full, name, tiling, ips):
+    """The bench's autotuned tiling (256 threads, packed mode 1) and the
+    library default (128 threads, mode 2) at every chunking the autotuner
+    times, at full size against the FP64 restatement."""
+    _check_full(full, name, tiling, ips)
 
 
 @pytest.mark.parametrize("mixed", [False, True])
