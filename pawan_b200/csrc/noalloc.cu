@@ -2,9 +2,8 @@
 // cannot allocate device memory.
 //
 // Who needs it: code that runs where cudaMalloc is not allowed or not safe --
-// inside a host callback or a region being captured into a CUDA graph by
-// someone else, under a memory manager that owns every allocation on the
-// device (a pool handed to a plugin), or in a hard real-time loop where an
+// inside a host callback, under a memory manager that owns every allocation on
+// the device (a pool handed to a plugin), or in a hard real-time loop where an
 // allocation's implicit synchronisation and latency are unacceptable.  Such a
 // caller owns its inputs and outputs but cannot let the library create
 // buffers.  This entry point therefore keeps all of its working memory (the
@@ -22,9 +21,15 @@
 // the caller.  Whatever must start at zero (the scheduler counter) is cleared
 // by the call itself; the rest is fully overwritten before it is read.
 //
-// The arithmetic is that of pawan_system_solve in PAWAN_PREC_F32 (same pair
-// kernel), with a fixed tiling (128 threads, one target per thread) and
-// 4,096-source chunks.
+// The pair kernel is pawan_system_solve's in PAWAN_PREC_F32 with the
+// high-order smoothing kernel only, at a fixed tiling (128 threads, one
+// target per thread) and 4,096-source chunks.  The FP32 positions are taken
+// relative to particle 0 (pawan_system_set_particles uses the centroid), and
+// the near-tile radius max(4 s_max, 0.03 x extent) measures the extent from
+// particle 0, so it can be up to twice the allocating path's: more tile pairs
+// may take the accurate near formulation.  Results therefore agree with
+// pawan_system_solve within the FP32 tolerance, not bit for bit.
+#include <cmath>
 #include <cstddef>
 #include <mutex>
 
@@ -130,8 +135,9 @@ __global__ void __launch_bounds__(kStageThreads)
   }
 }
 
-// One block: near-tile radius (as pawan_system_set_particles sets it), the
-// segment descriptor, the work list, and the cleared scheduler counter.
+// One block: near-tile radius (the rule of pawan_system_set_particles, with the
+// extent measured from particle 0), the segment descriptor, the work list, and
+// the cleared scheduler counter.
 __global__ void noalloc_plan(NoallocScratch *S, int n, int nblocks, double nu) {
   __shared__ float smax, emax;
   if (threadIdx.x == 0) {
@@ -232,7 +238,8 @@ extern "C" int pawan_interact_noalloc(const double *position, const double *vort
   using namespace pawan;
   if (!position || !vorticity || !radius || !volume || !velocity || !retvorcity)
     return PAWAN_ERR_INVALID;
-  if (n < 2 || n > (size_t)kNoallocMaxParticles || !(nu >= 0.0)) return PAWAN_ERR_INVALID;
+  if (n < 2 || n > (size_t)kNoallocMaxParticles || !std::isfinite(nu) || nu < 0.0)
+    return PAWAN_ERR_INVALID;
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return PAWAN_ERR_CUDA;
   DeviceSlot slot;
