@@ -13,14 +13,26 @@ import pytest
 import oracle
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = "/root/reference"
+
+
+def _reference_tree() -> str:
+    """The reference tree: $PAWAN_REF (as `make REF=...` takes it), else the
+    oracle Makefile's own default."""
+    if os.environ.get("PAWAN_REF"):
+        return os.environ["PAWAN_REF"]
+    r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-s", "--no-print-directory",
+                        "print-ref"], capture_output=True, text=True)
+    return r.stdout.strip() if r.returncode == 0 else ""
+
+
+REF = _reference_tree()
 needs_tree = pytest.mark.skipif(not os.path.isdir(os.path.join(REF, "src")),
                                 reason="reference tree absent")
 
 
 @needs_tree
 def test_oracle_host_code_is_clean_under_asan_and_ubsan():
-    r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-s", "sanitize"],
+    r = subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-s", f"REF={REF}", "sanitize"],
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr
     exe = os.path.join(ROOT, "oracle", "_ref", "sanitize_check")
