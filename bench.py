@@ -224,8 +224,9 @@ def state_update_roofline(prof_stage: dict) -> dict:
             "ms_per_launch": ms, "bytes_per_launch": prof_stage["stage_bytes"] / n,
             "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": (gbs / peak) if gbs else None,
             "peak_source": src,
-            "note": "the chunk partials it reads were just written by the pair kernel and are "
-                    "partly L2-resident, so frac can exceed 1"}
+            "bytes": "per particle: the 48-byte rates the pair kernel summed, the FP64 state vectors "
+                     "the stage reads and writes, radius and volume, and 128 bytes of packed tile data "
+                     "(336-384 bytes for an RK4 stage)"}
 
 
 def profiled_tiling_matches(tile: dict) -> bool:
@@ -253,6 +254,19 @@ def executed_from_profiles(tile: dict) -> dict:
 
 
 # ------------------------------------------------------------ CPU baseline
+
+def cpu_model() -> str:
+    """The host CPU's model name (as lscpu reports it), from /proc/cpuinfo."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.lower().startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
 
 def cpu_reference_sample(pos, vor, rad, vol, nu, target_s: float, cap_n: int = 16384):
     """Times the reference's OpenMP __parallel::solve() on the first n particles
@@ -312,7 +326,7 @@ def run_reference(args, rk: Ranks):
                        "precision": "fp64 (the reference's)", "parallelism": f"host threads x{threads}",
                        "sample_particles": n},
             "cpu_baseline": {"value": value, "unit": "G interactions/s", "cores": threads,
-                             "kind": "reference", "sample": sample},
+                             "cpu_model": cpu_model(), "kind": "reference", "sample": sample},
             "e2e": {"value": value, "unit": "G interactions/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -320,59 +334,168 @@ def run_reference(args, rk: Ranks):
 
 # ---------------------------------------------------- ragged batch leg
 
-def run_batch_leg(ctx, n_solves: int = 512, steps: int = 4, seed: int = 4) -> dict:
+def _increment_errors(finals, refs, initials) -> dict:
+    """Per-solve RMS / max relative error of the state increment (final state
+    minus initial state, the part the solve computes) against a reference
+    run's: worst, 90th percentile and median over the solves, and how many
+    exceed the RHS tolerance (1e-5 RMS)."""
+    from pawan_b200 import max_rel, rms_rel
+    rms = np.array([rms_rel(f - x0, r - x0) for f, r, x0 in zip(finals, refs, initials)])
+    mx = [max_rel(f - x0, r - x0) for f, r, x0 in zip(finals, refs, initials)]
+    return {"solves": len(rms), "rms_rel_max": float(rms.max()), "rms_rel_p90": float(np.percentile(rms, 90)),
+            "rms_rel_median": float(np.median(rms)), "max_rel_max": max(mx),
+            "solves_above_1e-5": int((rms > 1e-5).sum())}
+
+
+def _rhs_errors(rates, refs) -> dict:
+    """Per-solve RMS / max relative error of one right-hand side (u, dalpha)
+    against reference rates at the same state: worst and median."""
+    from pawan_b200 import error_stats
+    st = [error_stats(u, da, ur, dr) for (u, da), (ur, dr) in zip(rates, refs)]
+    out = {"solves": len(st)}
+    for k in ("u_rms_rel", "dalpha_rms_rel", "u_max_rel", "dalpha_max_rel"):
+        v = [x[k] for x in st]
+        out[k + "_worst"] = max(v)
+        if k.endswith("rms_rel"):
+            out[k + "_median"] = float(np.median(v))
+    return out
+
+
+TRAJECTORY_NOTE = ("state increments after several RK4 steps: the reference's singular kernel "
+                   "(q ~ 1/rho^3 inside the smoothing radius) makes some of these rings diverge within "
+                   "a few steps, and there any two roundings -- FP64 sums grouped differently included -- "
+                   "separate; the right-hand-side errors are the arithmetic's accuracy")
+
+
+def run_batch_leg(ctx, n_solves: int = 512, steps: int = 4, seed: int = 4, check_oracle: bool = True) -> dict:
     """512 independent single-ring solves (N log-uniform in [512, 16384]):
     `steps` RK4 steps of every solve as one batch (one persistent pair launch
     per stage, the step captured in a CUDA graph, tiles autotuned), against the
-    same steps run one solve per launch sequence.  solves/s = solves x
-    (steps / 100) per second, a solve being the workload's 100 steps."""
+    same steps run one solve per launch sequence -- each solve with its own
+    plan, the tiling autotuned per size class (half an octave of N) and its
+    step replayed from a CUDA graph, so the ratio measures batching alone --
+    and, for reference, one solve per launch with the library's default tiling
+    and no graph.  solves/s = solves x (steps / 100) per second, a solve being
+    the workload's 100 steps.  Accuracy: one right-hand side at the initial
+    states, batched against one solve per launch (every solve), against the
+    FP64 path on the GPU (16 solves spread over N) and against the FP64 oracle
+    on the CPU (the 8 smallest, with check_oracle); then the same comparisons
+    of the states after the 1 + steps steps."""
     from pawan_b200 import Batch, System
     from pawan_b200 import geometry as g
     scs = g.ragged_batch(n_solves=n_solves, seed=seed)
     inter = sum(4.0 * sc.n * sc.n for sc in scs) * steps
     dt = scs[0].dt
+    initials = [sc.state() for sc in scs]
     batched = [System.from_scenario(ctx, sc, "f32") for sc in scs]
     b = Batch(ctx, batched)
     b.autotune()
+    b.solve()                         # one right-hand side at the initial states
+    rates_b = [x.union_rates() for x in batched]
     b.rk4(dt, 1, use_graph=True)      # capture + warm-up
     ctx.synchronize()
     ctx.mark(2)
     b.rk4(dt, steps, use_graph=True)
     ctx.mark(3)
     t_b = ctx.elapsed_ms(2, 3) * 1e-3
+    finals_b = [x.get_states() for x in batched]
     b.close()
-    for s in batched:
-        s.close()
-    solo = [System.from_scenario(ctx, sc, "f32") for sc in scs]
-    for s in solo:                    # each with its own plan, default tiling
-        s.rk4(dt, 1)
-    ctx.synchronize()
-    ctx.mark(2)
-    for s in solo:
-        s.rk4(dt, steps)
-    ctx.mark(3)
-    t_s = ctx.elapsed_ms(2, 3) * 1e-3
-    for s in solo:
-        s.close()
+    for x in batched:
+        x.close()
+
+    rates_s = []
+
+    def one_per_launch(tuned: bool):
+        solo = [System.from_scenario(ctx, sc, "f32") for sc in scs]
+        if tuned:
+            by_class = {}
+            for x, sc in zip(solo, scs):
+                key = int(2 * np.log2(sc.n))
+                if key in by_class:
+                    x.set_config(**by_class[key])
+                else:
+                    by_class[key] = x.autotune()
+                x.solve()
+                rates_s.append(x.union_rates())
+        for x in solo:
+            x.rk4(dt, 1, use_graph=tuned)   # plan (+ capture) and warm-up
+        ctx.synchronize()
+        ctx.mark(2)
+        for x in solo:
+            x.rk4(dt, steps, use_graph=tuned)
+        ctx.mark(3)
+        t = ctx.elapsed_ms(2, 3) * 1e-3
+        finals = [x.get_states() for x in solo]
+        for x in solo:
+            x.close()
+        return t, finals
+
+    t_s, finals_s = one_per_launch(True)
+    t_u, _ = one_per_launch(False)
+
+    order = np.argsort([sc.n for sc in scs])
+    sample = [int(order[k]) for k in np.linspace(0, len(scs) - 1, 16).astype(int)]
+    small = [int(i) for i in order[:8]]
+    rates64, f64 = [], []
+    for i in sample:
+        x = System.from_scenario(ctx, scs[i], "f64")
+        x.solve()
+        rates64.append(x.union_rates())
+        x.rk4(dt, 1 + steps)
+        f64.append(x.get_states())
+        x.close()
+    acc = {"rhs_vs_one_solve_per_launch": _rhs_errors(rates_b, rates_s),
+           "rhs_vs_fp64_gpu_sample": dict(_rhs_errors([rates_b[i] for i in sample], rates64),
+                                          N=[scs[i].n for i in sample])}
+    traj = {"vs_one_solve_per_launch": _increment_errors(finals_b, finals_s, initials),
+            "vs_fp64_gpu_sample": _increment_errors([finals_b[i] for i in sample], f64,
+                                                    [initials[i] for i in sample])}
+    if check_oracle:
+        try:
+            import oracle
+            from pawan_b200 import union_to_state
+            rates_or, refs = [], []
+            for i in small:
+                pos, vor, rad, vol = scs[i].union()
+                rates_or.append(oracle.pairs(pos, vor, rad, vol, scs[i].nu))
+                p1, v1 = oracle.rk4_step(pos, vor, rad, vol, scs[i].nu, dt, 1 + steps)
+                refs.append(union_to_state(scs[i].counts, p1, v1))
+            acc["rhs_vs_fp64_oracle_sample"] = dict(_rhs_errors([rates_b[i] for i in small], rates_or),
+                                                    N=[scs[i].n for i in small])
+            traj["vs_fp64_oracle_sample"] = _increment_errors([finals_b[i] for i in small], refs,
+                                                              [initials[i] for i in small])
+        except (OSError, ImportError) as e:
+            acc["rhs_vs_fp64_oracle_sample"] = f"unavailable: {e}"
+    acc["tolerance"] = {"rms_rel": 1e-5, "max_rel": 1e-4}
+    acc["trajectory_after_steps"] = dict(traj, steps=1 + steps, note=TRAJECTORY_NOTE)
+
     frac = steps / 100.0
     return {"solves": n_solves, "steps_timed": steps,
             "batched": {"solves_per_s": n_solves * frac / t_b, "G_interactions_per_s": inter / t_b / 1e9,
                         "seconds": t_b},
             "one_solve_per_launch": {"solves_per_s": n_solves * frac / t_s,
-                                     "G_interactions_per_s": inter / t_s / 1e9, "seconds": t_s},
-            "speedup": t_s / t_b}
+                                     "G_interactions_per_s": inter / t_s / 1e9, "seconds": t_s,
+                                     "how": "own plan per solve, tiling autotuned per half-octave of N, "
+                                            "RK4 step replayed from a CUDA graph"},
+            "one_solve_per_launch_default_tiling_no_graph": {
+                "solves_per_s": n_solves * frac / t_u, "G_interactions_per_s": inter / t_u / 1e9,
+                "seconds": t_u},
+            "speedup": t_s / t_b, "accuracy": acc}
 
 
 # -------------------------------------------------------------- serving leg
 
 def run_serving_leg(ctx, rate: float, duration: float, n_lo: int, n_hi: int, steps_lo: int,
                     steps_hi: int, budget: float, cap: float, max_active: int, max_queue: int,
-                    drain: float, seed: int = 5, policy: str = "fifo") -> dict:
+                    drain: float, seed: int = 5, policy: str = "fifo", accuracy_sample: int = 0) -> dict:
     """Replays a Poisson arrival trace against the continuous-batching server in
     real time.  Requests are built and submitted at their arrival times; when
     the server's queue is full an arrival is rejected without building it (the
     engine would reject it the same way).  After the arrival window the run
-    waits up to `drain` seconds for requests in flight."""
+    waits up to `drain` seconds for requests in flight.  With accuracy_sample
+    = k, k completed requests (spread over the completion order) are run again
+    alone after the leg -- as an FP32 system on its own and on the FP64 path --
+    and their served results compared with both."""
     from pawan_b200 import Server
     from pawan_b200 import geometry as g
     reqs = g.serving_requests(rate=rate, duration=duration, seed=seed, n_lo=n_lo, n_hi=n_hi,
@@ -400,7 +523,7 @@ def run_serving_leg(ctx, rate: float, duration: float, n_lo: int, n_hi: int, ste
             ids[rid] = r
     t_arrivals = time.perf_counter() - t0
     deadline = time.perf_counter() + drain
-    lat, done_inter = [], 0.0
+    lat, done_inter, finished = [], 0.0, []
     pending = dict(ids)
     first = True  # requests that finished during the arrival window count too
     while pending and (first or time.perf_counter() < deadline):
@@ -412,13 +535,16 @@ def run_serving_leg(ctx, rate: float, duration: float, n_lo: int, n_hi: int, ste
                 if out is not None:
                     lat.append(td - ts)
                     done_inter += 4.0 * r.scenario.meta["N"] ** 2 * r.scenario.steps
+                    if accuracy_sample:
+                        finished.append((r, out))
         time.sleep(0.01)
     elapsed = time.perf_counter() - t0
     st = srv.stats()
     srv.close()
     lat.sort()
     pct = (lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None)
-    return {"policy": policy, "rate_per_s": rate, "arrival_window_s": duration, "arrivals": len(reqs),
+    accuracy = serving_accuracy(ctx, finished, accuracy_sample) if accuracy_sample and finished else None
+    return {"accuracy": accuracy, "policy": policy, "rate_per_s": rate, "arrival_window_s": duration, "arrivals": len(reqs),
             "N_range": [n_lo, n_hi], "steps_range": [steps_lo, steps_hi],
             "budget_bytes": budget, "max_step_interactions": cap, "max_active": max_active,
             "max_queue": max_queue, "submitted": len(ids), "completed": len(lat),
@@ -430,6 +556,44 @@ def run_serving_leg(ctx, rate: float, duration: float, n_lo: int, n_hi: int, ste
                                "planning": st["plan_seconds"], "retirement": st["retire_seconds"]},
             "engine_iterations": int(st["iterations"]),
             "elapsed_s": elapsed, "arrival_replay_s": t_arrivals}
+
+
+def serving_accuracy(ctx, finished, k: int) -> dict:
+    """Served results of k completed requests against the same request run
+    alone (FP32, its own system and plan) and on the FP64 path, plus one
+    right-hand side of each at its initial state in FP32 against FP64."""
+    from pawan_b200 import System
+    from pawan_b200 import geometry as g
+    pick = [finished[i] for i in np.linspace(0, len(finished) - 1, min(k, len(finished))).astype(int)]
+    served, solo32, solo64, initials, sizes, rhs32, rhs64 = [], [], [], [], [], [], []
+    for r, out in pick:
+        wakes = g.request_wakes(r.scenario.meta)
+        counts = [w.n for w in wakes]
+        pos, vor = np.concatenate([w.pos for w in wakes]), np.concatenate([w.vor for w in wakes])
+        rad, vol = np.concatenate([w.rad for w in wakes]), np.concatenate([w.vol for w in wakes])
+        runs = []
+        for prec in ("f32", "f64"):
+            x = System(ctx, counts, r.scenario.nu, prec)
+            x.set_particles(pos, vor, rad, vol)
+            if not runs:
+                initials.append(x.get_states())
+            x.solve()
+            (rhs32 if prec == "f32" else rhs64).append(x.union_rates())
+            x.rk4(r.scenario.dt, r.scenario.steps)
+            runs.append(x.get_states())
+            x.close()
+        served.append(out)
+        solo32.append(runs[0])
+        solo64.append(runs[1])
+        sizes.append(int(sum(counts)))
+    return {"requests": len(pick), "N": sizes,
+            "served_vs_alone_fp32": dict(_increment_errors(served, solo32, initials),
+                                         metric="state increment of the served result against the same "
+                                                "request run alone (FP32, its own plan)"),
+            "rhs_fp32_vs_fp64_gpu": dict(_rhs_errors(rhs32, rhs64),
+                                         metric="one right-hand side at the request's initial state"),
+            "trajectory_vs_fp64_gpu": dict(_increment_errors(served, solo64, initials), note=TRAJECTORY_NOTE),
+            "tolerance": {"rms_rel": 1e-5, "max_rel": 1e-4}}
 
 
 # --------------------------------------------------------------- GPU arm
@@ -469,13 +633,19 @@ def run_pawan(args, rk: Ranks):
     clocks.start()
     ctx.profile(True)
     launches0 = ctx.launch_count
+    ms = 0.0
     ctx.mark(0)
     for _ in range(args.steps):
+        # the restore (device copy + repack of the initial geometry) and the L2
+        # flush (256 MiB write) sit between the step's own events
         s.restore()
+        ctx.mark(2)
         s.rk4(dt, 1)
-        ctx.flush_l2()  # evicts L2 between timed steps (256 MiB write, <0.1% of a step)
+        ctx.mark(3)
+        ctx.flush_l2()
+        ms += ctx.elapsed_ms(2, 3)
     ctx.mark(1)
-    ms = ctx.elapsed_ms(0, 1)
+    ms_bracket = ctx.elapsed_ms(0, 1)
     ctx.synchronize()
     launches = ctx.launch_count - launches0
     prof = ctx.profile_read()
@@ -501,6 +671,9 @@ def run_pawan(args, rk: Ranks):
                        "n_particles": N, "wakes": len(sc.counts), "precision": "fp32 pairs, fp64 accumulation+state",
                        "parallelism": f"replicas x{rk.world}", "l2": "flushed between timed steps (256 MiB write)",
                        "state": "restored to the initial geometry before every step (device copy)",
+                       "timing": "CUDA events around each RK4 step; the restore and the L2 flush between "
+                                 "steps are outside them",
+                       "ms_per_step_with_restore_and_flush": ms_bracket / args.steps,
                        "tile": tuned, "sm_count": info["sm_count"]},
             "gpu_launches": int(launches), "clocks": clk,
             "roofline": {"bound": "fp32", "achieved": achieved_tflops, "peak": peak_tflops,
@@ -517,8 +690,18 @@ def run_pawan(args, rk: Ranks):
             "state_update": state_update_roofline(prof_stage)}
 
     if not args.quick:
+        from pawan_b200 import error_stats, max_rel, rms_rel
+        # the timed tiling's results at the specified geometry: one RHS and one
+        # RK4 step from the initial state
+        s.restore()
+        s.solve()
+        u32, da32 = s.union_rates()
+        x0 = sc.state()
+        s.restore()
+        s.rk4(dt, 1)
+        step32 = s.get_states()
         # plain FP64 comparator and tuned FP64 on the same workload: one RHS each
-        cmp = {}
+        cmp, rates64, steps64 = {}, {}, {}
         for prec in ("f64_plain", "f64"):
             s64 = System.from_scenario(ctx, sc, prec)
             s64.solve()
@@ -527,6 +710,9 @@ def run_pawan(args, rk: Ranks):
             s64.solve()
             p64 = ctx.profile_read()
             ctx.profile(False)
+            rates64[prec] = s64.union_rates()
+            s64.rk4(dt, 1)
+            steps64[prec] = s64.get_states()
             t = p64["pair_ms"] * 1e-3
             cmp[prec] = {"value": N * N / t / 1e9, "unit": "G interactions/s", "pair_launch_ms": t * 1e3}
             s64.close()
@@ -536,6 +722,23 @@ def run_pawan(args, rk: Ranks):
                                  "speedup_vs_plain": f32_rate / cmp["f64_plain"]["value"],
                                  "speedup_vs_tuned_fp64": f32_rate / cmp["f64"]["value"]}
         line["peak_fp64_tflops"] = ctx.peak_fp64(1.0) / 1e3
+        line["accuracy"] = {
+            "tiling": tuned,
+            "tolerance": {"rms_rel": 1e-5, "max_rel": 1e-4},
+            "rhs_vs_fp64_plain_gpu": dict(error_stats(u32, da32, *rates64["f64_plain"]), particles=N,
+                                          reference="the reference formula term by term in FP64 on the "
+                                                    "GPU (pairs_plain_kernel), every particle"),
+            "rk4_step_increment": {
+                "fp32_vs_fp64_tuned_gpu": {"rms_rel": rms_rel(step32 - x0, steps64["f64"] - x0),
+                                           "max_rel": max_rel(step32 - x0, steps64["f64"] - x0)},
+                "fp64_plain_vs_fp64_tuned_gpu": {
+                    "rms_rel": rms_rel(steps64["f64_plain"] - x0, steps64["f64"] - x0),
+                    "max_rel": max_rel(steps64["f64_plain"] - x0, steps64["f64"] - x0)},
+                "note": "one RK4 step from the specified geometry; its stages evaluate the rates at "
+                        "states moved by 0.5-1 dt, where the singular near field amplifies any difference "
+                        "in the rates: the two FP64 kernels, whose right-hand sides agree to ~1e-13, show "
+                        "the amplification"},
+        }
 
         # end to end through the C ABI: pinned host state in, RK4 step, state out
         hin = ctx.pinned((6 * N,))
@@ -556,23 +759,38 @@ def run_pawan(args, rk: Ranks):
                        "path": "pawan_system_set_states (pinned host) -> pawan_system_rk4 -> pawan_system_get_states"}
 
         if rk.world == 1 and not args.no_suite:
-            line["batched"] = run_batch_leg(ctx)
+            line["batched"] = run_batch_leg(ctx, check_oracle=not args.no_cpu_baseline)
             # continuous batching at a capacity-matched load (request sizes scaled
             # down so latencies are observable in seconds), against serving the
             # same trace one request at a time
             cm = dict(rate=120.0, duration=8.0, n_lo=1024, n_hi=16384, steps_lo=5, steps_hi=20,
                       budget=120e9, cap=0.0, max_queue=0, drain=60.0)
-            line["served"] = {"capacity_matched": run_serving_leg(ctx, max_active=0, **cm),
+            line["served"] = {"capacity_matched": run_serving_leg(ctx, max_active=0, accuracy_sample=16, **cm),
                               "capacity_matched_one_at_a_time": run_serving_leg(ctx, max_active=1, **cm),
                               "specified_load": run_serving_leg(
                                   ctx, rate=200.0, duration=10.0, n_lo=1024, n_hi=262144, steps_lo=50,
                                   steps_hi=400, budget=120e9, cap=2e11, max_active=0, max_queue=64,
                                   drain=0.0)}
         if rk.rank == 0 and rk.world == 1 and not args.no_cpu_baseline:
+            # the oracle as the checker: 4,096 sampled targets summed over all N
+            # sources in FP64 on the host cores
+            try:
+                import oracle
+                t = np.sort(np.random.default_rng(0).choice(N, 4096, replace=False))
+                u_or, da_or = oracle.pairs(pos, vor, rad, vol, sc.nu, targets=t)
+                line["accuracy"]["rhs_vs_fp64_oracle_sampled"] = dict(
+                    error_stats(u32[t], da32[t], u_or, da_or), targets=len(t), sources=N,
+                    reference="FP64 C restatement of INTERACT/KERNEL (oracle/restate.c), itself "
+                              "checked against the reference's compiled sources")
+                up, dp = rates64["f64_plain"]
+                line["accuracy"]["fp64_plain_gpu_vs_oracle_sampled"] = error_stats(up[t], dp[t], u_or, da_or)
+            except (OSError, ImportError) as e:
+                line["accuracy"]["rhs_vs_fp64_oracle_sampled"] = f"unavailable: {e}"
             try:
                 rate, n, tsec, threads = cpu_reference_sample(pos, vor, rad, vol, sc.nu, 10.0)
                 line["cpu_baseline"] = {
-                    "value": rate / 1e9, "unit": "G interactions/s", "cores": threads, "kind": "reference",
+                    "value": rate / 1e9, "unit": "G interactions/s", "cores": threads,
+                    "cpu_model": cpu_model(), "kind": "reference",
                     "sample": f"one __parallel::solve() of the reference (OpenMP, compiled from its sources) "
                               f"on the first {n} particles of the ring pair, {tsec:.1f} s"}
             except Exception as e:  # the reference build may be absent on a fresh checkout
