@@ -54,7 +54,8 @@ typedef struct {
   int items_per_slot;     /* work items per resident block (source chunking) */
   int packed;             /* far tiles two sources per FP32x2 instruction: 1 with
                              1/rho^2 from the MUFU reciprocal, 2 from rsqrt
-                             squared; 0: one source per instruction */
+                             squared, 3 one of each per source pair; 0: one
+                             source per instruction */
 } pawan_tiling;
 
 typedef struct pawan_ctx pawan_ctx;
@@ -83,7 +84,7 @@ int pawan_ctx_profile_read(pawan_ctx *ctx, double *pair_ms, unsigned long long *
                            double *pair_interactions);
 /* The same for the per-particle stage kernel (RK4 stage update and repack):
  * summed time (ms), launches, and algorithmic HBM bytes (what each launch must
- * read and write: chunk partials, FP64 state vectors, packed tile data). */
+ * read and write: the summed rates, FP64 state vectors, packed tile data). */
 int pawan_ctx_profile_stage(pawan_ctx *ctx, double *stage_ms, unsigned long long *stage_launches,
                             double *stage_bytes);
 /* Timing marks on the context's stream (CUDA events, slots 0..15) and the

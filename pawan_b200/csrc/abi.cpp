@@ -17,7 +17,7 @@ size_t pawan_system::device_bytes() const {
          vol.bytes() + wake_id.bytes() + pos32.bytes() + vor32.bytes() + poslo.bytes() +
          vorlo.bytes() + pos64.bytes() +
          vor64.bytes() + diag_scratch.bytes() + diag_out.bytes() + Xc.bytes() + field.bytes() +
-         (plan ? plan->partial.bytes() : 0);
+         (plan ? plan->partial.bytes() + plan->rates.bytes() + plan->tile_count.bytes() : 0);
 }
 
 // =================================================================== C ABI

@@ -16,8 +16,11 @@
 //   pos64  double4[N]  (x, y, z, s)       packed FP64 data (FP64 kernels,
 //   vor64  double4[N]  (ax, ay, az, v)     diagnostics)
 //   boxes  float4[2 per source tile]  bounding box of each tile's hi positions
-//   partial double[C][6][N]  per source-chunk sums (u, dalpha) of the pair
-//                      kernel, reduced in fixed chunk order by the stage kernel
+//   partial double[T][C][6][tpb]  per (target tile, source chunk) sums (u,
+//                      dalpha) of the pair kernel: T target tiles of tpb
+//                      particles, C source chunks
+//   rates  double[6][N]  the chunks summed in chunk order (u, dalpha), written
+//                      by the pair kernel's block that completes a target tile
 #pragma once
 
 #include <cuda_runtime.h>
@@ -34,7 +37,9 @@ struct SegDesc {
   const double4 *pos64;
   const double4 *vor64;
   const float4 *boxes;  // [2 * ceil(n / tile)] (lo, hi) per source tile
-  double *partial;      // [nchunks][6][n]
+  double *partial;      // [ceil(n / tpb)][nchunks][6][tpb] (unused when nchunks == 1)
+  double *rates;        // [6][n]
+  int *tile_count;      // [ceil(n / tpb)] items of the tile done in this launch (0 between launches)
   int n;
   int nchunks;
   double nu;
@@ -60,8 +65,7 @@ struct StageItem {
 
 // What the stage kernel needs of one segment.
 struct StageDesc {
-  const double *partial;
-  int nchunks;
+  const double *rates;  // [6][n], the pair kernel's summed chunks
   int n;
   double *X;   // state x
   double *Xs;  // stage state x_s
@@ -93,7 +97,7 @@ struct StageDesc {
 };
 
 enum StageMode : int {
-  STAGE_RATES = 0,   // R = sum of partials
+  STAGE_RATES = 0,   // R = the rates
   STAGE_K1 = 1,      // k1 = r; x_s = k1*(dt/2) + x; pack x_s
   STAGE_K2 = 2,      // k2 = r; x_s = k2*(dt/2) + x; pack x_s
   STAGE_K3 = 3,      // k2 = k2 + r; x_s = r*dt + x; pack x_s
@@ -121,5 +125,78 @@ constexpr double kSqrtHalf = 0.70710678118654752440;     // 1/sqrt(2)
 // Block sizes.  Source tiles (and so bounding boxes) are 128 or 256
 // particles; stage blocks cover whole tiles.
 constexpr int kStageThreads = 256;
+
+
+#ifdef __CUDACC__
+// ---- per-item partial sums and their in-launch reduction -------------------
+//
+// A work item (target tile x source chunk) of a segment with nchunks > 1
+// stores its sums in its own slot, partial_slot(); when nchunks == 1 it
+// writes the rates directly.  After storing, every thread of the block calls
+// finish_item(): the item is counted for its target tile, and the block whose
+// item completes the tile sums the tile's slots in chunk order
+// (r = c0, r += c1, ...: the same order whichever block is last, so results
+// do not depend on scheduling) into rates[6][n], drops the slots' L2 lines
+// without writing them back to DRAM (discard.global.L2: they are never read
+// again; the next launch writes them afresh), and re-arms the tile's counter
+// to 0 for the next launch.  Slots are multiples of 128 bytes (tpb is a
+// multiple of 8) and the partial buffer is 128-byte aligned, so no line is
+// shared between tiles.
+__device__ __forceinline__ double *partial_slot(const SegDesc &sg, int t0, int chunk, int tpb) {
+  const size_t tile = (size_t)(t0 / tpb);
+  return sg.partial + ((tile * (size_t)sg.nchunks + (size_t)chunk) * 6) * (size_t)tpb;
+}
+
+__device__ __forceinline__ void discard_l2_line(const void *p) {
+  asm volatile("discard.global.L2 [%0], 128;" ::"l"(p) : "memory");
+}
+
+template <int NT>
+__device__ __forceinline__ void finish_item(const SegDesc &sg, int t0, int tpb, int *s_flag) {
+  __threadfence();  // this thread's slot stores, before the count below
+  __syncthreads();
+  const int tile = t0 / tpb;
+  if (threadIdx.x == 0) *s_flag = (atomicAdd(sg.tile_count + tile, 1) == sg.nchunks - 1);
+  __syncthreads();
+  if (!*s_flag) return;  // block-uniform
+  __threadfence();
+  const double *base = sg.partial + (size_t)tile * (size_t)sg.nchunks * 6 * (size_t)tpb;
+  const int nt = min(tpb, sg.n - t0);
+  const size_t n = (size_t)sg.n;
+  const size_t cstride = 6 * (size_t)tpb;
+  for (int u = threadIdx.x; u < 6 * tpb; u += NT) {
+    const int k = u / tpb, q = u - k * tpb;
+    if (q >= nt) continue;
+    const double *p = base + (size_t)k * tpb + q;
+    double r = __ldcg(p);
+    int c = 1;
+    // four chunks' loads in flight, summed in chunk order
+    for (; c + 4 <= sg.nchunks; c += 4) {
+      const double a = __ldcg(p + c * cstride), b = __ldcg(p + (c + 1) * cstride);
+      const double d = __ldcg(p + (c + 2) * cstride), e = __ldcg(p + (c + 3) * cstride);
+      r = __dadd_rn(__dadd_rn(__dadd_rn(__dadd_rn(r, a), b), d), e);
+    }
+    for (; c < sg.nchunks; ++c) r = __dadd_rn(r, __ldcg(p + c * cstride));
+    sg.rates[(size_t)k * n + (size_t)t0 + q] = r;
+  }
+  __syncthreads();  // every read of the slots is done
+  const size_t lines = (size_t)sg.nchunks * cstride * sizeof(double) / 128;
+  for (size_t l = threadIdx.x; l < lines; l += NT)
+    discard_l2_line(reinterpret_cast<const char *>(base) + 128 * l);
+  if (threadIdx.x == 0) sg.tile_count[tile] = 0;
+}
+
+// Where an item's six sums go: its slot (row stride tpb) or, for a segment of
+// one chunk, the rates themselves (row stride n); index by target - t0.
+struct ItemOut {
+  double *base;
+  size_t stride;
+};
+
+__device__ __forceinline__ ItemOut item_out(const SegDesc &sg, int t0, int chunk, int tpb) {
+  if (sg.nchunks == 1) return ItemOut{sg.rates + t0, (size_t)sg.n};
+  return ItemOut{partial_slot(sg, t0, chunk, tpb), (size_t)tpb};
+}
+#endif  // __CUDACC__
 
 }  // namespace pawan

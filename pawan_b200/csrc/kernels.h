@@ -48,7 +48,7 @@ cudaError_t pairs_plain_occupancy(const PairConfig &c, int kernel, int *blocks_p
 cudaError_t launch_pairs_plain(const PairConfig &c, int kernel, int grid, const WorkItem *items,
                                int n_items, const SegDesc *segs, int *next_item, cudaStream_t s);
 
-// Per-particle stage kernel (reduce partials, RK4 stage update, pack).
+// Per-particle stage kernel (RK4 stage update from the summed rates, pack).
 cudaError_t launch_stage(int mode, int n_blocks, const StageItem *items, const StageDesc *descs,
                          cudaStream_t s);
 

@@ -8,7 +8,8 @@
 // caller owns its inputs and outputs but cannot let the library create
 // buffers.  This entry point therefore keeps all of its working memory (the
 // packed FP32 tile data, tile bounding boxes, per-chunk partial sums, the
-// work list and the scheduler counter) in one file-scope device array,
+// work list, the per-tile counters, the summed rates and the scheduler
+// counter) in one file-scope device array,
 // `g_noalloc_scratch`, sized for at most kNoallocMaxParticles particles.
 // Every GPU that loads the library reserves that array until the process
 // exits.
@@ -18,8 +19,9 @@
 // first call before any stream capture.  Later calls only launch kernels.
 // All calls share the one array, so calls whose kernels overlap on the GPU
 // (different streams, different host threads) race and must be serialised by
-// the caller.  Whatever must start at zero (the scheduler counter) is cleared
-// by the call itself; the rest is fully overwritten before it is read.
+// the caller.  Whatever must start at zero (the scheduler counter and the
+// per-tile counters) is cleared by the call itself; the rest is fully
+// overwritten before it is read.
 //
 // The pair kernel is pawan_system_solve's in PAWAN_PREC_F32 with the
 // high-order smoothing kernel only, at a fixed tiling (128 threads, one
@@ -57,14 +59,17 @@ struct NoallocScratch {
   float4 poslo[kNoallocMaxParticles];
   float4 vorlo[kNoallocMaxParticles];
   float4 boxes[2 * kNaMaxTiles];
-  double partial[kNaMaxChunks * 6 * kNoallocMaxParticles];
+  double partial[kNaMaxTiles * kNaMaxChunks * 6 * kNaTB];  // [tile][chunk][6][128]
+  double rates[6 * kNoallocMaxParticles];                  // [6][n]
   float block_max[2 * kNaPrepBlocks];  // per prepare block: max s, max |x - x0|^2
   WorkItem items[kNaMaxItems];
+  int tile_count[kNaMaxTiles];
   SegDesc seg;
   int counter;
 };
 
-static_assert(offsetof(NoallocScratch, boxes) % 256 == 0 && offsetof(NoallocScratch, partial) % 256 == 0,
+static_assert(offsetof(NoallocScratch, boxes) % 256 == 0 && offsetof(NoallocScratch, partial) % 256 == 0 &&
+                  offsetof(NoallocScratch, rates) % 256 == 0,
               "scratch arrays on 256-byte boundaries");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoallocScratch)];
@@ -158,6 +163,8 @@ __global__ void noalloc_plan(NoallocScratch *S, int n, int nblocks, double nu) {
     d.vor64 = nullptr;
     d.boxes = S->boxes;
     d.partial = S->partial;
+    d.rates = S->rates;
+    d.tile_count = S->tile_count;
     d.n = n;
     d.nchunks = (n + kNaChunk - 1) / kNaChunk;
     d.nu = nu;
@@ -168,6 +175,7 @@ __global__ void noalloc_plan(NoallocScratch *S, int n, int nblocks, double nu) {
   __syncthreads();
   const int tiles = (n + kNaTB - 1) / kNaTB;
   const int chunks = (n + kNaChunk - 1) / kNaChunk;
+  for (int t = threadIdx.x; t < tiles; t += blockDim.x) S->tile_count[t] = 0;
   for (int it = threadIdx.x; it < tiles * chunks; it += blockDim.x) {
     const int c = it / tiles, tt = it % tiles;
     WorkItem w;
@@ -180,18 +188,14 @@ __global__ void noalloc_plan(NoallocScratch *S, int n, int nblocks, double nu) {
   }
 }
 
-// Sum the chunk partials in chunk order into the caller's N x 3 outputs.
+// The pair kernel's rates ([6][n], chunks summed in chunk order) into the
+// caller's N x 3 outputs.
 __global__ void noalloc_reduce(const NoallocScratch *S, int n, double *vel, double *dvor) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x;
   if (l >= n) return;
-  const int chunks = (n + kNaChunk - 1) / kNaChunk;
-  double r[6];
-  for (int k = 0; k < 6; ++k) r[k] = S->partial[(size_t)k * n + l];
-  for (int c = 1; c < chunks; ++c)
-    for (int k = 0; k < 6; ++k) r[k] += S->partial[((size_t)c * 6 + k) * n + l];
   for (int k = 0; k < 3; ++k) {
-    vel[3 * (size_t)l + k] = r[k];
-    dvor[3 * (size_t)l + k] = r[3 + k];
+    vel[3 * (size_t)l + k] = S->rates[(size_t)k * n + l];
+    dvor[3 * (size_t)l + k] = S->rates[(size_t)(3 + k) * n + l];
   }
 }
 

@@ -61,9 +61,9 @@
 // source chunk) from a counter; sources stream through a two-stage shared-memory
 // ring, each thread starting asynchronous copies (cp.async, no registers held)
 // of one source (four float4) for the next tile while the block computes the
-// current one.  The result of an item (u, dalpha in
-// FP64) goes to its chunk of the partial buffer, which the stage kernel
-// reduces in chunk order.
+// current one.  The result of an item (u, dalpha in FP64) goes to its slot of
+// the partial buffer; the block that completes a target tile sums the tile's
+// slots in chunk order into the rates (finish_item, device.cuh).
 #include <mutex>
 #include <set>
 #include <utility>
@@ -346,7 +346,18 @@ struct Target2 {
 
 __device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
 
-template <bool DIFF, bool UNI, bool RCP, int NSRC, int U, int KERN, bool NZ>
+// 1/rho^2 of a source pair on a uniform-radius tile, given ri = rho^-1:
+// RM = 1 from the MUFU reciprocal (two XU operations), RM = 2 as ri * ri (one
+// FMA-pipe FMUL2), RM = 3 one of each (a MUFU reciprocal for the first source,
+// a scalar multiply for the second), which splits the work between the pipes.
+template <int RM>
+__device__ __forceinline__ float2 inv_r2(float2 r2, float2 ri) {
+  if (RM == 1) return make_float2(rcp_approx(r2.x), rcp_approx(r2.y));
+  if (RM == 2) return __fmul2_rn(ri, ri);
+  return make_float2(rcp_approx(r2.x), ri.y * ri.y);
+}
+
+template <bool DIFF, bool UNI, int RM, int NSRC, int U, int KERN, bool NZ>
 __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
                                                 const float4 *__restrict__ f1,
                                                 const float4 *__restrict__ f2,
@@ -375,7 +386,7 @@ __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
         const float2 sr = __fadd2_rn(r2, s2u);
         const float2 y = make_float2(rcp_approx(sr.x), rcp_approx(sr.y));
         const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-        const float2 ri2 = RCP ? make_float2(rcp_approx(r2.x), rcp_approx(r2.y)) : __fmul2_rn(ri, ri);
+        const float2 ri2 = inv_r2<RM>(r2, ri);
         const float2 ph = __ffma2_rn(__fmul2_rn(h2, y), y, y);
         qh = __fmul2_rn(__fmul2_rn(ph, ri), ri2);
         nfh = __fmul2_rn(qh, ri2);
@@ -393,9 +404,8 @@ __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
       const float2 sr = __fadd2_rn(r2, s2u);
       const float2 w = make_float2(rsqrtf(sr.x), rsqrtf(sr.y));
       const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-      // 1/rho^2 from the MUFU reciprocal (RCP) or from one FMA-pipe multiply:
-      // which pipe has room depends on the instruction mix around the loop
-      const float2 ri2 = RCP ? make_float2(rcp_approx(r2.x), rcp_approx(r2.y)) : __fmul2_rn(ri, ri);
+      // which pipe has room for 1/rho^2 depends on the instruction mix
+      const float2 ri2 = inv_r2<RM>(r2, ri);
       const float2 y = __fmul2_rn(w, w);
       const float2 u = __fmul2_rn(h2, y);
       const float2 v = __fmul2_rn(u, w);
@@ -563,8 +573,8 @@ __device__ __forceinline__ bool far_tiles(float gap2, float4 slo, float4 shi, fl
 // Threads per target P > 1 split a tile's sources (R = 1); targets per thread
 // R > 1 reuse each source loaded from shared memory for R targets (P = 1);
 // PK > 0: the far path processes two sources per FP32x2 instruction (P = R =
-// 1), taking 1/rho^2 on uniform-radius tiles from the MUFU reciprocal (PK = 1)
-// or from rsqrt squared (PK = 2).
+// 1), taking 1/rho^2 on uniform-radius tiles from the MUFU reciprocal (PK = 1),
+// from rsqrt squared (PK = 2) or one of each per source pair (PK = 3).
 // MINB: blocks per SM the register allocation is bounded for (occupancy).
 // KERN: the smoothing kernel (SmoothingKernel); the uniform-radius
 // specialisation exists for the high-order kernel only.
@@ -586,7 +596,7 @@ __global__ void __launch_bounds__(TB, MINB)
   float4 *const svl = spl + 2 * TB;
   float4 *const fq = svl + 2 * TB;
   float2 *const fz = reinterpret_cast<float2 *>(fq + 10 * FQ);
-  __shared__ int s_item;
+  __shared__ int s_item, s_last;
   const int tid = threadIdx.x;
   const int g = tid % P;
   const int lt = tid / P;
@@ -724,13 +734,13 @@ __global__ void __launch_bounds__(TB, MINB)
                      *f3 = fq + (6 + buf) * FQ, *f4 = fq + (8 + buf) * FQ;
         const float2 *f5 = fz + buf * FQ;
         if (nz && uni)
-          tile_far_packed<DIFF, true, PK == 1, TB, U, KERN, true>(f0, f1, f2, f3, f4, f5, T2, slo.w, b);
+          tile_far_packed<DIFF, true, PK, TB, U, KERN, true>(f0, f1, f2, f3, f4, f5, T2, slo.w, b);
         else if (nz)
-          tile_far_packed<DIFF, false, PK == 1, TB, U, KERN, true>(f0, f1, f2, f3, f4, f5, T2, 0.f, b);
+          tile_far_packed<DIFF, false, PK, TB, U, KERN, true>(f0, f1, f2, f3, f4, f5, T2, 0.f, b);
         else if (uni)
-          tile_far_packed<DIFF, true, PK == 1, TB, U, KERN, false>(f0, f1, f2, f3, f4, f5, T2, slo.w, b);
+          tile_far_packed<DIFF, true, PK, TB, U, KERN, false>(f0, f1, f2, f3, f4, f5, T2, slo.w, b);
         else
-          tile_far_packed<DIFF, false, PK == 1, TB, U, KERN, false>(f0, f1, f2, f3, f4, f5, T2, 0.f, b);
+          tile_far_packed<DIFF, false, PK, TB, U, KERN, false>(f0, f1, f2, f3, f4, f5, T2, 0.f, b);
         const double s2 = uni ? 2.0 * (double)slo.w : 1.0;
         const double As2 = A * s2;
         const double cd = uni ? 32.0 * cnu : cnu;
@@ -835,20 +845,21 @@ __global__ void __launch_bounds__(TB, MINB)
       }
     }
 
+    const ItemOut o = item_out(sg, w.t0, w.chunk, TPB);
     if (g == 0) {
-      const size_t n = (size_t)sg.n;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         if (!valid[r]) continue;
-        double *out = sg.partial + (size_t)w.chunk * 6 * n + ti[r];
+        double *out = o.base + (ti[r] - w.t0);
         out[0] = ou[r][0];
-        out[n] = ou[r][1];
-        out[2 * n] = ou[r][2];
-        out[3 * n] = oa[r][0];
-        out[4 * n] = oa[r][1];
-        out[5 * n] = oa[r][2];
+        out[o.stride] = ou[r][1];
+        out[2 * o.stride] = ou[r][2];
+        out[3 * o.stride] = oa[r][0];
+        out[4 * o.stride] = oa[r][1];
+        out[5 * o.stride] = oa[r][2];
       }
     }
+    if (sg.nchunks > 1) finish_item<TB>(sg, w.t0, TPB, &s_last);
   }
 }
 
@@ -878,6 +889,9 @@ KernelFn select_highorder(const PairConfig &c) {
   PAWAN_F32_CASE_PK(128, 1, 1, 4, 3, 2)
   PAWAN_F32_CASE_PK(128, 1, 1, 8, 3, 2)
   PAWAN_F32_CASE_PK(256, 1, 1, 8, 2, 2)
+  PAWAN_F32_CASE_PK(256, 1, 1, 4, 2, 3)
+  PAWAN_F32_CASE_PK(256, 1, 1, 2, 2, 3)
+  PAWAN_F32_CASE_PK(128, 1, 1, 4, 4, 3)
   PAWAN_F32_CASE(128, 1, 1, 2, 4)
   PAWAN_F32_CASE(128, 1, 1, 4, 4)
   PAWAN_F32_CASE(128, 2, 1, 2, 4)

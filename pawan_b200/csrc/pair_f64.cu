@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(TB)
                      const SegDesc *__restrict__ segs, int *__restrict__ next_item) {
   __shared__ double4 sp[2][TB];
   __shared__ double4 sv[2][TB];
-  __shared__ int s_item;
+  __shared__ int s_item, s_last;
   const int tid = threadIdx.x;
 
   for (;;) {
@@ -151,15 +151,16 @@ __global__ void __launch_bounds__(TB)
         day += c * ey;
         daz += c * ez;
       }
-      const size_t n = (size_t)sg.n;
-      double *out = sg.partial + (size_t)w.chunk * 6 * n + i;
+      const ItemOut o = item_out(sg, w.t0, w.chunk, TB);
+      double *out = o.base + (i - w.t0);
       out[0] = A * ux;
-      out[n] = A * uy;
-      out[2 * n] = A * uz;
-      out[3 * n] = dax;
-      out[4 * n] = day;
-      out[5 * n] = daz;
+      out[o.stride] = A * uy;
+      out[2 * o.stride] = A * uz;
+      out[3 * o.stride] = dax;
+      out[4 * o.stride] = day;
+      out[5 * o.stride] = daz;
     }
+    if (sg.nchunks > 1) finish_item<TB>(sg, w.t0, TB, &s_last);
   }
 }
 

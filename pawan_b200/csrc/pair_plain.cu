@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(TB)
                        const SegDesc *__restrict__ segs, int *__restrict__ next_item) {
   __shared__ double4 sp[TB];
   __shared__ double4 sv[TB];
-  __shared__ int s_item;
+  __shared__ int s_item, s_last;
   const int tid = threadIdx.x;
   const double one_over_pi = kInvPi;
 
@@ -104,15 +104,16 @@ __global__ void __launch_bounds__(TB)
     }
 
     if (valid) {
-      const size_t n = (size_t)sg.n;
-      double *out = sg.partial + (size_t)w.chunk * 6 * n + i;
+      const ItemOut o = item_out(sg, w.t0, w.chunk, TB);
+      double *out = o.base + (i - w.t0);
       out[0] = u0;
-      out[n] = u1;
-      out[2 * n] = u2;
-      out[3 * n] = a0;
-      out[4 * n] = a1;
-      out[5 * n] = a2;
+      out[o.stride] = u1;
+      out[2 * o.stride] = u2;
+      out[3 * o.stride] = a0;
+      out[4 * o.stride] = a1;
+      out[5 * o.stride] = a2;
     }
+    if (sg.nchunks > 1) finish_item<TB>(sg, w.t0, TB, &s_last);
   }
 }
 

@@ -153,8 +153,12 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     double cost;
   };
   std::vector<ItemCost> items;
-  size_t partial_total = 0, box_total = 0;
+  // per system: partial slots [target tiles][chunks][6][TPB] (none with one
+  // chunk), rates [6][n], one counter per target tile
+  if (TPB % 8 != 0) return fail(ctx, PAWAN_ERR_INVALID, "targets per block must be a multiple of 8");
+  size_t partial_total = 0, box_total = 0, rates_total = 0, count_total = 0;
   std::vector<size_t> partial_off(systems.size()), box_off(systems.size());
+  std::vector<size_t> rates_off(systems.size()), count_off(systems.size());
   p->nchunks.resize(systems.size());
   for (size_t s = 0; s < systems.size(); ++s) {
     const int n = (int)systems[s]->n;
@@ -165,8 +169,13 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     tiles_per_chunk = std::max(1, std::min(tiles_per_chunk, src_tiles));
     const int nch = (src_tiles + tiles_per_chunk - 1) / tiles_per_chunk;
     p->nchunks[s] = nch;
+    const size_t target_tiles = ((size_t)n + TPB - 1) / TPB;
     partial_off[s] = partial_total;
-    partial_total += (size_t)nch * 6 * (size_t)n;
+    if (nch > 1) partial_total += target_tiles * (size_t)nch * 6 * (size_t)TPB;
+    rates_off[s] = rates_total;
+    rates_total += 6 * (size_t)n;
+    count_off[s] = count_total;
+    count_total += target_tiles;
     box_off[s] = box_total;
     box_total += 2 * (size_t)src_tiles;
     // targets: all particles, or this process's block of a sharded system
@@ -190,6 +199,8 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
 
   if (ordered_alloc) {
     p->partial.ordered_on(ctx->stream);
+    p->rates.ordered_on(ctx->stream);
+    p->tile_count.ordered_on(ctx->stream);
     p->boxes.ordered_on(ctx->stream);
     p->items.ordered_on(ctx->stream);
     p->segs.ordered_on(ctx->stream);
@@ -198,6 +209,9 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     p->stage_descs.ordered_on(ctx->stream);
   }
   PAWAN_CUDA(ctx, p->partial.alloc(partial_total));
+  PAWAN_CUDA(ctx, p->rates.alloc(rates_total));
+  PAWAN_CUDA(ctx, p->tile_count.alloc(count_total));
+  PAWAN_CUDA(ctx, cudaMemsetAsync(p->tile_count.p, 0, p->tile_count.bytes(), ctx->stream));
   PAWAN_CUDA(ctx, p->boxes.alloc(box_total));
   std::vector<WorkItem> wh(items.size());
   p->item_costs.resize(items.size());
@@ -218,14 +232,15 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     d.pos64 = y->pos64.p;
     d.vor64 = y->vor64.p;
     d.boxes = p->boxes.p + box_off[s];
-    d.partial = p->partial.p + partial_off[s];
+    d.partial = p->nchunks[s] > 1 ? p->partial.p + partial_off[s] : nullptr;
+    d.rates = p->rates.p + rates_off[s];
+    d.tile_count = p->tile_count.p + count_off[s];
     d.n = (int)y->n;
     d.nchunks = p->nchunks[s];
     d.nu = y->nu;
     d.near2 = (float)(y->r_near * y->r_near);
     StageDesc &g = p->stage_host[s];
-    g.partial = d.partial;
-    g.nchunks = d.nchunks;
+    g.rates = d.rates;
     g.n = d.n;
     g.X = y->X.p;
     g.Xs = y->Xs.p;
@@ -370,16 +385,17 @@ static void note_repack(Plan &p) {
   }
 }
 
-// Algorithmic HBM bytes of one stage launch: per particle the chunk partials
-// (or the gathered rates of a sharded system), the FP64 state vectors the mode
-// reads and writes, radius and volume, and the 128 bytes of packed FP32 / FP64
-// tile data; 32 bytes of bounding box per tile.
+// Algorithmic HBM bytes of one stage launch: per particle the rates (48
+// bytes: the pair kernel's summed chunks, or the gathered rates of a sharded
+// system), the FP64 state vectors the mode reads and writes, radius and
+// volume, and the 128 bytes of packed FP32 / FP64 tile data; 32 bytes of
+// bounding box per tile.  An RK4 stage is 336-384 bytes per particle.
 static double stage_bytes(const Plan &p, int mode) {
   double total = 0.0;
   for (size_t s = 0; s < p.systems.size(); ++s) {
     const pawan_system *y = p.systems[s];
     const double n = (double)y->n;
-    const double rates = y->shard.active ? 48.0 : 48.0 * (double)p.nchunks[s];
+    const double rates = 48.0;
     const double pack = 16.0 + 128.0 + 32.0 / (double)p.tile.pc.tb;
     double per = 0.0;
     switch (mode) {

@@ -166,7 +166,9 @@ struct Plan {
   int n_stage_blocks = 0;
   double interactions = 0.0;  // sum n^2
   std::vector<int> nchunks;
-  DBuf<double> partial;
+  DBuf<double> partial;   // per system [target tiles][chunks][6][tpb] (chunks > 1)
+  DBuf<double> rates;     // per system [6][n]: the summed chunks
+  DBuf<int> tile_count;   // per system and target tile; 0 between launches
   DBuf<float4> boxes;
   DBuf<WorkItem> items;
   DBuf<SegDesc> segs;

@@ -24,7 +24,9 @@
 // turns at about one target of work per iteration.  Small requests
 // then keep their pace beside arbitrarily large ones, as with chunked
 // prefill in language-model serving.  Its result is unchanged, bit for bit:
-// every work item writes its own partial slot whichever launch runs it.
+// every work item writes its own partial slot whichever launch runs it, and
+// a target tile's slots are summed in chunk order by the item that completes
+// the tile, in whichever launch that is.
 //
 // The engine's systems and plans take their device memory from the device's
 // memory pool in the order of the engine's stream (cudaMallocAsync /
@@ -85,12 +87,14 @@ struct Request {
 };
 
 // Device bytes a request holds while active: the system's buffers plus its
-// partial chunks in a batched plan (fixed chunk size).
+// rates and partial slots in a batched plan (fixed chunk size; slots cover
+// whole target tiles of at most 512 particles).
 double request_bytes(size_t n, int tb) {
-  const double per = 5 * 48.0 + 16.0 + 4.0 + 64.0 + 64.0 + 1.0;
+  const double per = 5 * 48.0 + 16.0 + 4.0 + 64.0 + 64.0 + 1.0 + 48.0;
   const size_t chunk = ((kServeChunkSources + tb - 1) / tb) * (size_t)tb;
   const size_t nch = (n + chunk - 1) / chunk;
-  return (double)n * per + 48.0 * (double)n * (double)nch + 4096.0;
+  const double slots = nch > 1 ? 48.0 * (double)(n + 512) * (double)nch : 0.0;
+  return (double)n * per + slots + 4096.0;
 }
 
 }  // namespace
@@ -152,8 +156,9 @@ int plan_iteration(pawan_server *srv, std::vector<Request *> &act, std::unique_p
 // A slice of a large request's stage work, about `budget` interactions (at
 // least one work item per resident block of the pair kernel, so the slice
 // fills the device; on into the following stages while the budget lasts).
-// Each work item writes its own partial slot, so splitting a stage over
-// launches changes nothing in the result.  Adds the interactions done to *work.
+// Each work item writes its own partial slot and the tile counters carry over
+// between launches, so splitting a stage over launches changes nothing in the
+// result.  Adds the interactions done to *work.
 int large_slice(pawan_server *srv, Request *r, double budget, double *work) {
   static const int modes[4] = {STAGE_K1, STAGE_K2, STAGE_K3, STAGE_FINAL};
   pawan_ctx *ctx = srv->ctx;

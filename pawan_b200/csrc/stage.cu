@@ -1,8 +1,8 @@
-// Per-particle stage kernel: reduces the pair kernel's partial chunks in fixed
-// chunk order into the rates (u | dalpha), applies the RK4 stage update in
-// FP64 with the reference's operation order, packs the new state into the
-// FP32 hi/lo and FP64 tile arrays the next pair launch reads, and writes the
-// bounding box of each source tile.  One thread per particle, HBM-bound.
+// Per-particle stage kernel: reads the rates (u | dalpha) the pair kernel
+// summed, applies the RK4 stage update in FP64 with the reference's operation
+// order, packs the new state into the FP32 hi/lo and FP64 tile arrays the next
+// pair launch reads, and writes the bounding box of each source tile.  One
+// thread per particle, HBM-bound.
 //
 // Reference: __rk4::step (src/integration/rk4.cpp:12-76):
 //   x1 = k1*(0.5 dt) + x        (:29-31)      STAGE_K1
@@ -21,14 +21,10 @@
 namespace pawan {
 namespace {
 
-// Partial chunks loaded per batch, and blocks per SM the register budget is
-// held to: a segment of 131,072 particles is 512 blocks of 256, one wave at
-// four blocks per SM on 148 SMs.  The descriptor is read through a reference
-// (uniform, L1-cached) rather than copied, which is what frees the registers.
-// Measured at N = 131,072 with 16 chunks: batch 1 or 2 at 64 registers
-// 28.6 us per launch; batch 3 or 4 (spilling at 64, or 80-85 registers and
-// three blocks per SM) 30-34 us; batch 8 at 134 registers 37 us.
-constexpr int kStageChunkBatch = 2;
+// Blocks per SM the register budget is held to: a segment of 131,072
+// particles is 512 blocks of 256, one wave at four blocks per SM on 148 SMs.
+// The descriptor is read through a reference (uniform, L1-cached) rather than
+// copied, which is what frees the registers.
 constexpr int kStageMinBlocks = 4;
 
 // Packs one particle: FP32 hi/lo pairs of the position relative to the
@@ -109,29 +105,10 @@ __global__ void __launch_bounds__(kStageThreads, kStageMinBlocks)
 #pragma unroll
       for (int k = 0; k < 6; ++k) r[k] = g[(size_t)k * S];
     } else {
-      // Chunks are summed in order (r = c0, then r += c1, c2, ...), but
-      // loaded kStageChunkBatch at a time, the last batch partly, so that
-      // each thread keeps 6 x kStageChunkBatch loads in flight: the kernel is
-      // bound by memory latency, not by its few adds.  The partials are read
-      // once; streaming loads keep them from evicting the state from L2.
-      for (int c0 = 0; c0 < d.nchunks; c0 += kStageChunkBatch) {
-        double v[kStageChunkBatch][6];
+      // the pair kernel's rates (its chunks already summed); read once, so
+      // streaming loads keep them from evicting the state from L2
 #pragma unroll
-        for (int u = 0; u < kStageChunkBatch; ++u) {
-          if (c0 + u < d.nchunks) {
-            const double *p = d.partial + (size_t)(c0 + u) * 6 * n + l;
-#pragma unroll
-            for (int k = 0; k < 6; ++k) v[u][k] = __ldcs(p + (size_t)k * n);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < kStageChunkBatch; ++u) {
-          if (c0 + u < d.nchunks) {
-#pragma unroll
-            for (int k = 0; k < 6; ++k) r[k] = (c0 + u == 0) ? v[u][k] : __dadd_rn(r[k], v[u][k]);
-          }
-        }
-      }
+      for (int k = 0; k < 6; ++k) r[k] = __ldcs(d.rates + (size_t)k * n + l);
     }
   }
   if (MODE == STAGE_SHARD) {
