@@ -54,8 +54,7 @@ typedef struct {
   int items_per_slot;     /* work items per resident block (source chunking) */
   int packed;             /* far tiles two sources per FP32x2 instruction: 1 with
                              1/rho^2 from the MUFU reciprocal, 2 from rsqrt
-                             squared, 3 one of each per source pair; 0: one
-                             source per instruction */
+                             squared; 0: one source per instruction */
 } pawan_tiling;
 
 typedef struct pawan_ctx pawan_ctx;

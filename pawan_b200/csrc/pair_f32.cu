@@ -348,13 +348,12 @@ __device__ __forceinline__ float2 bc2(float v) { return make_float2(v, v); }
 
 // 1/rho^2 of a source pair on a uniform-radius tile, given ri = rho^-1:
 // RM = 1 from the MUFU reciprocal (two XU operations), RM = 2 as ri * ri (one
-// FMA-pipe FMUL2), RM = 3 one of each (a MUFU reciprocal for the first source,
-// a scalar multiply for the second), which splits the work between the pipes.
+// FMA-pipe FMUL2).  (One of each per pair was measured too: slower than both
+// on the ring pair, the helical wake and the ragged batch.)
 template <int RM>
 __device__ __forceinline__ float2 inv_r2(float2 r2, float2 ri) {
   if (RM == 1) return make_float2(rcp_approx(r2.x), rcp_approx(r2.y));
-  if (RM == 2) return __fmul2_rn(ri, ri);
-  return make_float2(rcp_approx(r2.x), ri.y * ri.y);
+  return __fmul2_rn(ri, ri);
 }
 
 template <bool DIFF, bool UNI, int RM, int NSRC, int U, int KERN, bool NZ>
@@ -573,8 +572,8 @@ __device__ __forceinline__ bool far_tiles(float gap2, float4 slo, float4 shi, fl
 // Threads per target P > 1 split a tile's sources (R = 1); targets per thread
 // R > 1 reuse each source loaded from shared memory for R targets (P = 1);
 // PK > 0: the far path processes two sources per FP32x2 instruction (P = R =
-// 1), taking 1/rho^2 on uniform-radius tiles from the MUFU reciprocal (PK = 1),
-// from rsqrt squared (PK = 2) or one of each per source pair (PK = 3).
+// 1), taking 1/rho^2 on uniform-radius tiles from the MUFU reciprocal (PK = 1)
+// or from rsqrt squared (PK = 2).
 // MINB: blocks per SM the register allocation is bounded for (occupancy).
 // KERN: the smoothing kernel (SmoothingKernel); the uniform-radius
 // specialisation exists for the high-order kernel only.
@@ -889,9 +888,6 @@ KernelFn select_highorder(const PairConfig &c) {
   PAWAN_F32_CASE_PK(128, 1, 1, 4, 3, 2)
   PAWAN_F32_CASE_PK(128, 1, 1, 8, 3, 2)
   PAWAN_F32_CASE_PK(256, 1, 1, 8, 2, 2)
-  PAWAN_F32_CASE_PK(256, 1, 1, 4, 2, 3)
-  PAWAN_F32_CASE_PK(256, 1, 1, 2, 2, 3)
-  PAWAN_F32_CASE_PK(128, 1, 1, 4, 4, 3)
   PAWAN_F32_CASE(128, 1, 1, 2, 4)
   PAWAN_F32_CASE(128, 1, 1, 4, 4)
   PAWAN_F32_CASE(128, 2, 1, 2, 4)

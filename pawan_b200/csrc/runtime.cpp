@@ -114,8 +114,10 @@ static size_t shard_count(const pawan_system *y) {
 // Work decomposition.  Target tiles of tb/p particles; sources in chunks of
 // whole tb-tiles sized so that the launch holds about `items_per_slot` items
 // per resident block (or of `fixed_chunk_sources` when > 0, which makes a
-// system's arithmetic independent of the other systems in the plan).  Items are ordered largest first, so the dynamic
-// counter hands out the long ones early (longest-processing-time order).
+// system's arithmetic independent of the other systems in the plan).  The
+// systems with the largest items come first, so the dynamic counter hands out
+// the long items early (longest-processing-time order), and within a system a
+// target tile's chunks are consecutive.
 int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int precision,
                const TileChoice &tile, std::unique_ptr<Plan> &out, int fixed_chunk_sources,
                bool ordered_alloc) {
@@ -159,6 +161,7 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
   size_t partial_total = 0, box_total = 0, rates_total = 0, count_total = 0;
   std::vector<size_t> partial_off(systems.size()), box_off(systems.size());
   std::vector<size_t> rates_off(systems.size()), count_off(systems.size());
+  std::vector<double> sys_cost(systems.size(), 0.0);
   p->nchunks.resize(systems.size());
   for (size_t s = 0; s < systems.size(); ++s) {
     const int n = (int)systems[s]->n;
@@ -183,17 +186,25 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     const pawan_system *y = systems[s];
     const int t_lo = y->shard.active ? (int)shard_first(y) : 0;
     const int t_hi = y->shard.active ? t_lo + (int)shard_count(y) : n;
-    for (int c = 0; c < nch; ++c) {
-      const int s0 = c * tiles_per_chunk * TB;
-      const int s1 = std::min(n, (c + 1) * tiles_per_chunk * TB);
-      for (int t0 = t_lo; t0 < t_hi; t0 += TPB) {
-        const int nt = std::min(TPB, t_hi - t0);
-        items.push_back({WorkItem{(int)s, t0, c, s0, s1}, (double)nt * (double)(s1 - s0)});
+    // target-major: a target tile's chunks are consecutive, so they run at
+    // about the same time and the block completing the tile finds their
+    // partial slots still in L2
+    for (int t0 = t_lo; t0 < t_hi; t0 += TPB) {
+      const int nt = std::min(TPB, t_hi - t0);
+      for (int c = 0; c < nch; ++c) {
+        const int s0 = c * tiles_per_chunk * TB;
+        const int s1 = std::min(n, (c + 1) * tiles_per_chunk * TB);
+        const double cost = (double)nt * (double)(s1 - s0);
+        sys_cost[s] = std::max(sys_cost[s], cost);
+        items.push_back({WorkItem{(int)s, t0, c, s0, s1}, cost});
       }
     }
   }
-  std::stable_sort(items.begin(), items.end(),
-                   [](const ItemCost &a, const ItemCost &b) { return a.cost > b.cost; });
+  // Systems whose items are largest go first (longest-processing-time order
+  // across the systems of a batch); each system's items keep their order.
+  std::stable_sort(items.begin(), items.end(), [&](const ItemCost &a, const ItemCost &b) {
+    return sys_cost[a.w.seg] > sys_cost[b.w.seg];
+  });
   if (items.size() > (size_t)INT32_MAX) return fail(ctx, PAWAN_ERR_INVALID, "too many work items");
   p->n_items = (int)items.size();
 
