@@ -230,10 +230,12 @@ def state_update_roofline(prof_stage: dict) -> dict:
 
 
 def profiled_tiling_matches(tile: dict) -> bool:
-    """Whether the committed ncu summary was captured with this tiling (its
-    traffic and pipe figures depend on it: chunking sets the partial-sum bytes)."""
+    """Whether the committed ncu summary was captured with this tiling: its
+    pipe and traffic figures depend on the block shape and far-path mode.  The
+    chunking (items per resident block) is not compared: the chunk sums stay in
+    L2 inside the launch, so the DRAM bytes do not depend on it."""
     prof = profile_summary().get("tile")
-    return bool(prof) and all(tile.get(k) == v for k, v in prof.items())
+    return bool(prof) and all(tile.get(k) == v for k, v in prof.items() if k != "items_per_slot")
 
 
 def traffic_from_profiles(tile: dict):

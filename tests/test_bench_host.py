@@ -14,12 +14,14 @@ def test_profile_figures_apply_only_to_the_profiled_tiling():
     prof = bench.profile_summary()
     if not prof.get("tile"):
         pytest.skip("no committed ncu summary")
-    tile = dict(prof["tile"])
+    tile = dict(prof["tile"], items_per_slot=64)
     assert bench.profiled_tiling_matches(tile)
+    # the chunking does not change the DRAM bytes (chunk sums stay in L2)
+    assert bench.profiled_tiling_matches(dict(tile, items_per_slot=128))
     assert bench.traffic_from_profiles(tile) == prof["dram_bytes_per_launch_full_size"]
     ex = bench.executed_from_profiles(tile)
     assert ex["same_tiling"] and ex["profiled_kernel"] == prof["kernel"]
-    other = dict(tile, items_per_slot=tile["items_per_slot"] // 2)
+    other = dict(tile, packed=2 if tile["packed"] != 2 else 1)
     assert not bench.profiled_tiling_matches(other)
     assert bench.traffic_from_profiles(other) is None
     assert bench.executed_from_profiles(other)["same_tiling"] is False
