@@ -382,29 +382,13 @@ __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
     if (NZ) {
       // Z-free far field in pairs (kernel_scalars_nz), no diffusion sums
       if (UNI) {
-        if (RM == 4) {
-          // one MUFU per source: with e = sigma^2 / rho^2 <= 1/36 on these
-          // tiles, ph = y (1 + h y) = ri2 f(e), f = (1 + 1.5 e) / (1 + e)^2 =
-          // 1 - e/2 + e^3/2 - e^4 + O(1.5 e^5 <= 2.5e-8)
-          const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-          const float2 ri2 = __fmul2_rn(ri, ri);
-          const float2 e = __fmul2_rn(s2u, ri2);
-          const float2 e2 = __fmul2_rn(e, e);
-          const float2 a = __ffma2_rn(bc2(-1.f), e, bc2(0.5f));
-          const float2 b = __ffma2_rn(e2, a, bc2(-0.5f));
-          const float2 f = __ffma2_rn(e, b, bc2(1.f));
-          const float2 ri5 = __fmul2_rn(__fmul2_rn(ri, ri2), ri2);
-          qh = __fmul2_rn(ri5, f);
-          nfh = __fmul2_rn(qh, ri2);
-        } else {
-          const float2 sr = __fadd2_rn(r2, s2u);
-          const float2 y = make_float2(rcp_approx(sr.x), rcp_approx(sr.y));
-          const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-          const float2 ri2 = inv_r2<RM>(r2, ri);
-          const float2 ph = __ffma2_rn(__fmul2_rn(h2, y), y, y);
-          qh = __fmul2_rn(__fmul2_rn(ph, ri), ri2);
-          nfh = __fmul2_rn(qh, ri2);
-        }
+        const float2 sr = __fadd2_rn(r2, s2u);
+        const float2 y = make_float2(rcp_approx(sr.x), rcp_approx(sr.y));
+        const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+        const float2 ri2 = inv_r2<RM>(r2, ri);
+        const float2 ph = __ffma2_rn(__fmul2_rn(h2, y), y, y);
+        qh = __fmul2_rn(__fmul2_rn(ph, ri), ri2);
+        nfh = __fmul2_rn(qh, ri2);
       } else {
         const float2 sig2 = __fadd2_rn(T.h, hj);
         float qa, fa, qb, fb;
@@ -904,8 +888,6 @@ KernelFn select_highorder(const PairConfig &c) {
   PAWAN_F32_CASE_PK(128, 1, 1, 4, 3, 2)
   PAWAN_F32_CASE_PK(128, 1, 1, 8, 3, 2)
   PAWAN_F32_CASE_PK(256, 1, 1, 8, 2, 2)
-  PAWAN_F32_CASE_PK(256, 1, 1, 4, 2, 4)
-  PAWAN_F32_CASE_PK(128, 1, 1, 4, 4, 4)
   PAWAN_F32_CASE(128, 1, 1, 2, 4)
   PAWAN_F32_CASE(128, 1, 1, 4, 4)
   PAWAN_F32_CASE(128, 2, 1, 2, 4)
