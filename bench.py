@@ -342,11 +342,17 @@ def _increment_errors(finals, refs, initials) -> dict:
     run's: worst, 90th percentile and median over the solves, and how many
     exceed the RHS tolerance (1e-5 RMS)."""
     from pawan_b200 import max_rel, rms_rel
-    rms = np.array([rms_rel(f - x0, r - x0) for f, r, x0 in zip(finals, refs, initials)])
-    mx = [max_rel(f - x0, r - x0) for f, r, x0 in zip(finals, refs, initials)]
-    return {"solves": len(rms), "rms_rel_max": float(rms.max()), "rms_rel_p90": float(np.percentile(rms, 90)),
-            "rms_rel_median": float(np.median(rms)), "max_rel_max": max(mx),
-            "solves_above_1e-5": int((rms > 1e-5).sum())}
+    finite = [bool(np.all(np.isfinite(f)) and np.all(np.isfinite(r))) for f, r in zip(finals, refs)]
+    pairs = [(f, r, x0) for f, r, x0, ok in zip(finals, refs, initials, finite) if ok]
+    out = {"solves": len(finals), "non_finite": len(finals) - len(pairs)}
+    if not pairs:
+        return out
+    rms = np.array([rms_rel(f - x0, r - x0) for f, r, x0 in pairs])
+    mx = [max_rel(f - x0, r - x0) for f, r, x0 in pairs]
+    out.update({"rms_rel_max": float(rms.max()), "rms_rel_p90": float(np.percentile(rms, 90)),
+                "rms_rel_median": float(np.median(rms)), "max_rel_max": max(mx),
+                "solves_above_1e-5": int((rms > 1e-5).sum())})
+    return out
 
 
 def _rhs_errors(rates, refs) -> dict:

@@ -51,34 +51,47 @@ __device__ __forceinline__ float4 pack(const StageDesc &d, int l, const double x
 // Bounding boxes of the block's tiles (box_tile particles each, aligned to
 // the segment); particles beyond n contribute nothing.  The box's w components
 // carry the tile's smallest (lo) and largest (hi) h = s^2/2, so the pair
-// kernel can tell tile pairs of one smoothing radius.
+// kernel can tell tile pairs of one smoothing radius.  Each warp reduces its
+// 32 particles by shuffles, then one thread per tile combines the tile's
+// warps (4 or 8) from shared memory: one barrier.
 __device__ __forceinline__ void tile_boxes(const StageDesc &d, int l0, float4 p, bool has) {
-  __shared__ float lo[4][kStageThreads];
-  __shared__ float hi[4][kStageThreads];
-  const int t = threadIdx.x;
-  lo[0][t] = has ? p.x : INFINITY;
-  lo[1][t] = has ? p.y : INFINITY;
-  lo[2][t] = has ? p.z : INFINITY;
-  lo[3][t] = has ? p.w : INFINITY;
-  hi[0][t] = has ? p.x : -INFINITY;
-  hi[1][t] = has ? p.y : -INFINITY;
-  hi[2][t] = has ? p.z : -INFINITY;
-  hi[3][t] = has ? p.w : -INFINITY;
+  constexpr int kWarps = kStageThreads / 32;
+  __shared__ float wv[8][kWarps];
+  float v[8] = {has ? p.x : INFINITY,  has ? p.y : INFINITY,  has ? p.z : INFINITY,
+                has ? p.w : INFINITY,  has ? p.x : -INFINITY, has ? p.y : -INFINITY,
+                has ? p.z : -INFINITY, has ? p.w : -INFINITY};
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      v[k] = fminf(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+      v[4 + k] = fmaxf(v[4 + k], __shfl_xor_sync(0xffffffffu, v[4 + k], o));
+    }
+  }
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) wv[k][warp] = v[k];
+  }
   __syncthreads();
-  for (int s = d.box_tile / 2; s > 0; s >>= 1) {
-    if ((t % d.box_tile) < s) {
+  const int wpt = d.box_tile / 32;
+  if (t < kStageThreads / d.box_tile && l0 + t * d.box_tile < d.n) {
+    float lo[4], hi[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      lo[k] = wv[k][t * wpt];
+      hi[k] = wv[4 + k][t * wpt];
+    }
+    for (int w = 1; w < wpt; ++w) {
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
-        lo[k][t] = fminf(lo[k][t], lo[k][t + s]);
-        hi[k][t] = fmaxf(hi[k][t], hi[k][t + s]);
+        lo[k] = fminf(lo[k], wv[k][t * wpt + w]);
+        hi[k] = fmaxf(hi[k], wv[4 + k][t * wpt + w]);
       }
     }
-    __syncthreads();
-  }
-  if ((t % d.box_tile) == 0 && l0 + t < d.n) {
-    const int b = (l0 + t) / d.box_tile;
-    d.boxes[2 * b] = make_float4(lo[0][t], lo[1][t], lo[2][t], lo[3][t]);
-    d.boxes[2 * b + 1] = make_float4(hi[0][t], hi[1][t], hi[2][t], hi[3][t]);
+    const int b = (l0 + t * d.box_tile) / d.box_tile;
+    d.boxes[2 * b] = make_float4(lo[0], lo[1], lo[2], lo[3]);
+    d.boxes[2 * b + 1] = make_float4(hi[0], hi[1], hi[2], hi[3]);
   }
 }
 
