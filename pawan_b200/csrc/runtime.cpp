@@ -11,6 +11,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdint>
 #include <cstring>
 #include <numeric>
 
@@ -220,6 +221,10 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     p->stage_descs.ordered_on(ctx->stream);
   }
   PAWAN_CUDA(ctx, p->partial.alloc(partial_total));
+  // the pair kernels discard the slots' L2 lines after summing them: every
+  // slot must start on a 128-byte line (slot sizes are multiples of 128 bytes)
+  if (reinterpret_cast<uintptr_t>(p->partial.p) % 128 != 0)
+    return fail(ctx, PAWAN_ERR_CUDA, "partial-sum buffer not 128-byte aligned");
   PAWAN_CUDA(ctx, p->rates.alloc(rates_total));
   PAWAN_CUDA(ctx, p->tile_count.alloc(count_total));
   PAWAN_CUDA(ctx, cudaMemsetAsync(p->tile_count.p, 0, p->tile_count.bytes(), ctx->stream));
