@@ -370,3 +370,33 @@ def test_tile_classes_at_their_boundaries(ctx, gap, mixed):
         du, dda = (ug2 - ug1)[:n], (dag2 - dag1)[:n]
         assert rms_rel(du, du_ref) < 1e-5 and rms_rel(dda, dda_ref) < 1e-5, \
             (cfg, rms_rel(du, du_ref), rms_rel(dda, dda_ref))
+
+
+@pytest.mark.parametrize("tiling", [TIMED_TILING, DEFAULT_TILING, (128, 2, 1, 4, 0, 0), (128, 1, 2, 2, 0, 0)],
+                         ids=["timed", "default", "two-threads-per-target", "two-targets-per-thread"])
+def test_chunk_sums_inside_the_launch(ctx, tiling):
+    """The pair kernels sum a target tile's chunk partials inside the launch
+    (the block completing the tile, in chunk order).  With the tiling fixed,
+    the chunking changes only how the FP64 sums are grouped -- every FP32
+    tile sum is the same -- so plans of 1 to 1,024 work items per resident
+    block (from a few source chunks per target tile to one per source tile)
+    agree to FP64 rounding; a chunk lost or counted twice would differ by
+    percents.  Also across repeated launches (the tile counters re-arm) and a
+    ragged last tile.  (A single chunk, where items write the rates directly,
+    is the small systems of test_ragged_sizes_against_restatement.)"""
+    sc = g.ring_pair(n_stations=300, seed=61, nu=1e-4)  # N = 4,800: ragged target tiles
+    tb, p, r, unroll, minb, mode = tiling
+    s = System.from_scenario(ctx, sc, "f32")
+    results = []
+    for ips in (1, 2, 8, 32, 128, 1024):
+        s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=mode)
+        s.solve()
+        first = s.union_rates()
+        s.solve()
+        again = s.union_rates()
+        assert np.array_equal(first[0], again[0]) and np.array_equal(first[1], again[1])
+        results.append(first)
+    u0, d0 = results[0]
+    for u, d in results[1:]:
+        assert rms_rel(u, u0) < 1e-13 and rms_rel(d, d0) < 1e-13, (rms_rel(u, u0), rms_rel(d, d0))
+    s.close()
