@@ -65,7 +65,7 @@ def parse():
                          "one replica per rank")
     ap.add_argument("--tile", default=None,
                     help="fixed FP32 tiling instead of the autotuned one: threads,threads_per_target,"
-                         "targets_per_thread,unroll,blocks_per_sm,packed[,items_per_slot]")
+                         "targets_per_thread,unroll,blocks_per_sm,packed[,items_per_slot[,split_near]]")
     return ap.parse_args()
 
 
@@ -73,7 +73,8 @@ def apply_tile(s, spec: str):
     v = [int(x) for x in spec.split(",")]
     tb, p, r, unroll, minb, packed = v[:6]
     ips = v[6] if len(v) > 6 else 32
-    s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=packed)
+    split = v[7] if len(v) > 7 else 0
+    s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=packed, split_near=split)
     return s.get_config()
 
 

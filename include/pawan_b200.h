@@ -55,6 +55,10 @@ typedef struct {
   int packed;             /* far tiles two sources per FP32x2 instruction: 1 with
                              1/rho^2 from the MUFU reciprocal, 2 from rsqrt
                              squared; 0: one source per instruction */
+  int split_near;         /* FP32: 1 computes the near tile pairs in a pass of
+                             their own before the far pass (each kernel with its
+                             own registers; faster where near pairs are many);
+                             0: one pass */
 } pawan_tiling;
 
 typedef struct pawan_ctx pawan_ctx;

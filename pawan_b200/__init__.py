@@ -58,16 +58,17 @@ class ServeConfig(ctypes.Structure):
 class Tiling(ctypes.Structure):
     _fields_ = [("threads", ctypes.c_int), ("threads_per_target", ctypes.c_int),
                 ("targets_per_thread", ctypes.c_int), ("unroll", ctypes.c_int),
-                ("blocks_per_sm", ctypes.c_int), ("items_per_slot", ctypes.c_int), ("packed", ctypes.c_int)]
+                ("blocks_per_sm", ctypes.c_int), ("items_per_slot", ctypes.c_int), ("packed", ctypes.c_int),
+                ("split_near", ctypes.c_int)]
 
 
 def _tiling(threads, threads_per_target=1, unroll=4, items_per_slot=16, targets_per_thread=1,
-            blocks_per_sm=0, packed=0) -> Tiling:
+            blocks_per_sm=0, packed=0, split_near=0) -> Tiling:
     """packed: 0 one source per instruction on far tiles; 1 two sources per FP32x2
     instruction with 1/rho^2 from the MUFU reciprocal; 2 the same with 1/rho^2
     from rsqrt squared (True means 1)."""
     return Tiling(threads, threads_per_target, targets_per_thread, unroll, blocks_per_sm, items_per_slot,
-                  int(packed))
+                  int(packed), int(split_near))
 
 
 class ServeStats(ctypes.Structure):
@@ -451,9 +452,9 @@ class System:
 
     def set_config(self, threads: int, threads_per_target: int = 1, unroll: int = 4,
                    items_per_slot: int = 16, targets_per_thread: int = 1, blocks_per_sm: int = 0,
-                   packed: int = 0):
+                   packed: int = 0, split_near: int = 0):
         t = _tiling(threads, threads_per_target, unroll, items_per_slot, targets_per_thread, blocks_per_sm,
-                    packed)
+                    packed, split_near)
         self.ctx.check(self._lib.pawan_system_set_tiling(self._h, ctypes.byref(t)))
 
     def get_config(self) -> dict:
@@ -510,9 +511,9 @@ class Batch:
 
     def set_config(self, threads: int, threads_per_target: int = 1, unroll: int = 4,
                    items_per_slot: int = 16, targets_per_thread: int = 1, blocks_per_sm: int = 0,
-                   packed: int = 0):
+                   packed: int = 0, split_near: int = 0):
         t = _tiling(threads, threads_per_target, unroll, items_per_slot, targets_per_thread, blocks_per_sm,
-                    packed)
+                    packed, split_near)
         self.ctx.check(self._lib.pawan_batch_set_tiling(self._h, ctypes.byref(t)))
 
     def autotune(self):

@@ -147,7 +147,7 @@ int pawan_ctx_create(int device, pawan_ctx **out) {
   if (prop.major != 10) return PAWAN_ERR_CUDA;  // built for sm_100a only
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
     return PAWAN_ERR_CUDA;
-  if (cudaMalloc(&ctx->d_counter, sizeof(int)) != cudaSuccess) {
+  if (cudaMalloc(&ctx->d_counter, 2 * sizeof(int)) != cudaSuccess) {
     cudaStreamDestroy(ctx->stream);
     return PAWAN_ERR_NOMEM;
   }
@@ -635,9 +635,10 @@ static int tile_from_abi(pawan_ctx *ctx, int precision, int kernel, const pawan_
   if (!t) return fail(ctx, PAWAN_ERR_INVALID, "null tiling");
   TileChoice c;
   c.pc = PairConfig{t->threads, t->threads_per_target, t->unroll, t->targets_per_thread,
-                    t->blocks_per_sm, t->packed};
+                    t->blocks_per_sm, t->packed, t->split_near};
   c.items_per_slot = t->items_per_slot;
   if (t->items_per_slot < 1 || t->targets_per_thread < 1 || t->blocks_per_sm < 0 || t->packed < 0 ||
+      t->split_near < 0 || (t->split_near > 0 && precision != PAWAN_PREC_F32) ||
       !tile_supported(precision, c.pc, kernel))
     return fail(ctx, PAWAN_ERR_INVALID, "tiling not compiled for this precision and kernel");
   *out = c;
@@ -662,6 +663,7 @@ int pawan_system_get_tiling(pawan_system *sys, pawan_tiling *tiling) {
   tiling->unroll = sys->tile.pc.unroll;
   tiling->blocks_per_sm = sys->tile.pc.minb;
   tiling->packed = sys->tile.pc.packed;
+  tiling->split_near = sys->tile.pc.split;
   tiling->items_per_slot = sys->tile.items_per_slot;
   return PAWAN_OK;
 }
@@ -679,6 +681,7 @@ int pawan_tile_candidates(int precision, int kernel, pawan_tiling *out, size_t c
     out[i].unroll = v[i].pc.unroll;
     out[i].blocks_per_sm = v[i].pc.minb;
     out[i].packed = v[i].pc.packed;
+    out[i].split_near = v[i].pc.split;
     out[i].items_per_slot = v[i].items_per_slot;
   }
   return PAWAN_OK;

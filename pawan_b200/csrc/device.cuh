@@ -40,6 +40,10 @@ struct SegDesc {
   double *partial;      // [ceil(n / tpb)][nchunks][6][tpb] (unused when nchunks == 1)
   double *rates;        // [6][n]
   int *tile_count;      // [ceil(n / tpb)] items of the tile done in this launch (0 between launches)
+  // with a separate near pass (split tilings): each item's sums over its near
+  // tile pairs, [ceil(n / tpb)][nchunks][6][tpb], and whether it had any
+  double *near_partial;
+  unsigned char *near_flag;  // [ceil(n / tpb)][nchunks]
   int n;
   int nchunks;
   double nu;

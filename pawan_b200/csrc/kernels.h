@@ -14,6 +14,10 @@ namespace pawan {
 // `packed` = far tiles computed two sources per FP32x2 instruction (1: 1/rho^2
 // from the MUFU reciprocal on uniform-radius tiles, 2: from rsqrt squared;
 // 0: one source per instruction).
+// `split` = 1: near tile pairs are computed by a pass of their own before the
+// far pass (which then skips them), each kernel with its own register
+// allocation, the near pass forming alpha_i x alpha_j by the projection form
+// (19 operations instead of the one pass's 27).
 struct PairConfig {
   int tb;
   int p;
@@ -21,6 +25,7 @@ struct PairConfig {
   int r = 1;
   int minb = 0;
   int packed = 0;
+  int split = 0;
 };
 
 inline int targets_per_block(const PairConfig &c) { return c.tb / c.p * c.r; }
@@ -30,6 +35,7 @@ inline int targets_per_block(const PairConfig &c) { return c.tb / c.p * c.r; }
 // FP32 pair math, FP64 accumulation of per-tile partial sums.
 bool pairs_f32_supported(const PairConfig &c, int kernel);
 cudaError_t pairs_f32_occupancy(const PairConfig &c, bool diffusion, int kernel, int *blocks_per_sm);
+// next_item: two counters (the far pass's and the near pass's), zero at launch.
 cudaError_t launch_pairs_f32(const PairConfig &c, bool diffusion, int kernel, int grid,
                              const WorkItem *items, int n_items, const SegDesc *segs,
                              int *next_item, cudaStream_t s);

@@ -165,6 +165,8 @@ __global__ void noalloc_plan(NoallocScratch *S, int n, int nblocks, double nu) {
     d.partial = S->partial;
     d.rates = S->rates;
     d.tile_count = S->tile_count;
+    d.near_partial = nullptr;
+    d.near_flag = nullptr;
     d.n = n;
     d.nchunks = (n + kNaChunk - 1) / kNaChunk;
     d.nu = nu;

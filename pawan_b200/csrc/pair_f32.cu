@@ -481,9 +481,32 @@ __device__ __forceinline__ void cross_accurate(float ax, float ay, float az, flo
   wz = det2(ax, ay, bx, by) + fmaf(ax, my, fmaf(-ay, mx, fmaf(lx, by, -ly * bx)));
 }
 
+// (a + a_lo) x (b + b_lo) for a target strength a + a_lo and a source strength
+// b + b_lo (FP32 hi + lo), accurate to a few ulp of the result also for nearly
+// parallel or antiparallel strengths, in 19 operations (cross_accurate: 27).
+// With mu = (a.b)/|a|^2, v = b - mu a is formed by one FMA per component, so
+// exactly up to its own rounding, and a x v = a x b whatever mu's rounding
+// (its error only moves v along a).  v is (nearly) perpendicular to a, so
+// a x (v + b_lo) has no cancellation; and a_lo x b = mu (a_lo x a) + a_lo x v,
+// the last term eps |a||v| relative to |a x v| = |a||v|.  iaa = 1/|a|^2 (0
+// for a = 0) and (lx, ly, lz) = a_lo x a are per target.
+__device__ __forceinline__ void projection_cross(float ax, float ay, float az, float iaa, float lx,
+                                                 float ly, float lz, float bx, float by, float bz,
+                                                 float mx, float my, float mz, float &wx, float &wy,
+                                                 float &wz) {
+  const float mu = fmaf(az, bz, fmaf(ay, by, ax * bx)) * iaa;
+  const float vx = fmaf(-mu, ax, bx) + mx;
+  const float vy = fmaf(-mu, ay, by) + my;
+  const float vz = fmaf(-mu, az, bz) + mz;
+  wx = fmaf(mu, lx, fmaf(ay, vz, -az * vy));
+  wy = fmaf(mu, ly, fmaf(az, vx, -ax * vz));
+  wz = fmaf(mu, lz, fmaf(ax, vy, -ay * vx));
+}
+
 // Near tile, shared-memory format: sp, sv, spl, svl = pos32, vor32, poslo,
 // vorlo of the sources; tpl, tvl = poslo, vorlo of the targets.
-template <bool DIFF, bool CHECK, int P, int R, int NSRC, int KERN>
+// NX: alpha_i x alpha_j by cross_accurate (0) or projection_cross (1).
+template <bool DIFF, bool CHECK, int P, int R, int NSRC, int KERN, int NX = 0>
 __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
                                           const float4 *__restrict__ sv,
                                           const float4 *__restrict__ spl,
@@ -491,6 +514,17 @@ __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
                                           const int (&skip)[R], const Target (&T)[R],
                                           const float4 (&tpl)[R], const float4 (&tvl)[R],
                                           Acc32 (&a)[R]) {
+  float iaa[R], lcx[R], lcy[R], lcz[R];  // per target, for projection_cross
+  if (NX) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const float aa = fmaf(T[r].ch, T[r].ch, fmaf(T[r].bh, T[r].bh, T[r].ah * T[r].ah));
+      iaa[r] = aa > 0.f ? 1.0f / aa : 0.f;
+      lcx[r] = fmaf(tvl[r].y, T[r].ch, -tvl[r].z * T[r].bh);
+      lcy[r] = fmaf(tvl[r].z, T[r].ah, -tvl[r].x * T[r].ch);
+      lcz[r] = fmaf(tvl[r].x, T[r].bh, -tvl[r].y * T[r].ah);
+    }
+  }
   // near tiles are a few percent of the work: no unrolling keeps the register
   // budget of the far loop
 #pragma unroll 1
@@ -521,8 +555,12 @@ __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
       const float cz = fmaf(s.x, dy, -s.y * dx);
       // stretching: alpha_i x alpha_j from the hi/lo strengths
       float wx, wy, wz;
-      cross_accurate(T[r].ah, T[r].bh, T[r].ch, tvl[r].x, tvl[r].y, tvl[r].z, s.x, s.y, s.z, sl.x,
-                     sl.y, sl.z, wx, wy, wz);
+      if (NX)
+        projection_cross(T[r].ah, T[r].bh, T[r].ch, iaa[r], lcx[r], lcy[r], lcz[r], s.x, s.y, s.z,
+                         sl.x, sl.y, sl.z, wx, wy, wz);
+      else
+        cross_accurate(T[r].ah, T[r].bh, T[r].ch, tvl[r].x, tvl[r].y, tvl[r].z, s.x, s.y, s.z, sl.x,
+                       sl.y, sl.z, wx, wy, wz);
       const float t = fmaf(dz, wz, fmaf(dy, wy, dx * wx));
       float ft = fh * t;
       if (CHECK) {
@@ -577,7 +615,9 @@ __device__ __forceinline__ bool far_tiles(float gap2, float4 slo, float4 shi, fl
 // MINB: blocks per SM the register allocation is bounded for (occupancy).
 // KERN: the smoothing kernel (SmoothingKernel); the uniform-radius
 // specialisation exists for the high-order kernel only.
-template <int TB, int P, int R, int U, bool DIFF, int MINB, int PK, int KERN>
+// SPLIT: near tile pairs were computed by pairs_f32_near_kernel before this
+// launch; they are skipped here and each item adds its near sums (if any).
+template <int TB, int P, int R, int U, bool DIFF, int MINB, int PK, int KERN, bool SPLIT = false>
 __global__ void __launch_bounds__(TB, MINB)
     pairs_f32_kernel(const WorkItem *__restrict__ items, int n_items,
                      const SegDesc *__restrict__ segs, int *__restrict__ next_item) {
@@ -800,7 +840,7 @@ __global__ void __launch_bounds__(TB, MINB)
             oa[r][2] += cd * (v * a[r].ez - (double)a[r].ev * az[r]);
           }
         }
-      } else {
+      } else if (!SPLIT) {
         int skip[R];
         float4 tpl[R], tvl[R];
 #pragma unroll
@@ -844,6 +884,21 @@ __global__ void __launch_bounds__(TB, MINB)
       }
     }
 
+    if (SPLIT) {
+      const size_t fi = (size_t)(w.t0 / TPB) * (size_t)sg.nchunks + (size_t)w.chunk;
+      if (sg.near_flag[fi] && g == 0) {
+        const double *ns = sg.near_partial + fi * 6 * (size_t)TPB;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int q = ti[r] - w.t0;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            ou[r][k] += ns[(size_t)k * TPB + q];
+            oa[r][k] += ns[(size_t)(3 + k) * TPB + q];
+          }
+        }
+      }
+    }
     const ItemOut o = item_out(sg, w.t0, w.chunk, TPB);
     if (g == 0) {
 #pragma unroll
@@ -862,16 +917,168 @@ __global__ void __launch_bounds__(TB, MINB)
   }
 }
 
+// The near pass of a split tiling: the same work items, only their near tile
+// pairs (the same box test as pairs_f32_kernel), each staged and computed
+// with the accurate near formulation; an item's sums go to its near slot and
+// its flag says whether it had any.  It runs before the far pass, which adds
+// the flagged slots to its own sums.
+template <int TB, int P, int R, bool DIFF, int MINB, int KERN, int NX>
+__global__ void __launch_bounds__(TB, MINB)
+    pairs_f32_near_kernel(const WorkItem *__restrict__ items, int n_items,
+                          const SegDesc *__restrict__ segs, int *__restrict__ next_item) {
+  constexpr int TG = TB / P;
+  constexpr int TPB = TG * R;
+  __shared__ float4 sp[TB], sv[TB], spl[TB], svl[TB];
+  __shared__ int s_item;
+  const int tid = threadIdx.x;
+  const int g = tid % P;
+  const int lt = tid / P;
+  const double A = kInv4Pi;
+
+  for (;;) {
+    if (tid == 0) s_item = atomicAdd(next_item, 1);
+    __syncthreads();
+    const int it = s_item;
+    __syncthreads();
+    if (it >= n_items) break;
+
+    const WorkItem w = items[it];
+    const SegDesc sg = segs[w.seg];
+    const double cnu = 15.0 * sg.nu * A;
+    int ti[R];
+    bool valid[R];
+    Target T[R];
+    float4 tpl[R], tvl[R];
+    double ou[R][3], oa[R][3], ax[R], ay[R], az[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      ti[r] = w.t0 + lt + r * TG;
+      valid[r] = ti[r] < sg.n;
+      float4 a = make_float4(0.f, 0.f, 0.f, 1.f), b = make_float4(0.f, 0.f, 0.f, 0.f);
+      tpl[r] = tvl[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (valid[r]) {
+        a = __ldg(sg.pos32 + ti[r]);
+        b = __ldg(sg.vor32 + ti[r]);
+        tpl[r] = __ldg(sg.poslo + ti[r]);
+        tvl[r] = __ldg(sg.vorlo + ti[r]);
+      }
+      T[r].xh = a.x; T[r].yh = a.y; T[r].zh = a.z; T[r].h = a.w;
+      T[r].ah = b.x; T[r].bh = b.y; T[r].ch = b.z; T[r].v = b.w;
+      ax[r] = (double)b.x + (double)tvl[r].x;
+      ay[r] = (double)b.y + (double)tvl[r].y;
+      az[r] = (double)b.z + (double)tvl[r].z;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) ou[r][k] = oa[r][k] = 0.0;
+    }
+    float4 tlo = __ldg(sg.boxes + 2 * (w.t0 / TB));
+    float4 thi = __ldg(sg.boxes + 2 * (w.t0 / TB) + 1);
+#pragma unroll
+    for (int q = 1; q < (TPB + TB - 1) / TB; ++q) {
+      if (w.t0 + q * TB < sg.n) {
+        const float4 l2 = __ldg(sg.boxes + 2 * (w.t0 / TB + q));
+        const float4 h2 = __ldg(sg.boxes + 2 * (w.t0 / TB + q) + 1);
+        tlo = make_float4(fminf(tlo.x, l2.x), fminf(tlo.y, l2.y), fminf(tlo.z, l2.z),
+                          fminf(tlo.w, l2.w));
+        thi = make_float4(fmaxf(thi.x, h2.x), fmaxf(thi.y, h2.y), fmaxf(thi.z, h2.z),
+                          fmaxf(thi.w, h2.w));
+      }
+    }
+
+    bool any = false;
+    const int ntiles = (w.s1 - w.s0 + TB - 1) / TB;
+    for (int t = 0; t < ntiles; ++t) {
+      const int ts = w.s0 + t * TB;
+      const float4 slo = __ldg(sg.boxes + 2 * (ts / TB));
+      const float4 shi = __ldg(sg.boxes + 2 * (ts / TB) + 1);
+      const bool diag = (ts < w.t0 + TPB) && (w.t0 < ts + TB);
+      const bool near = diag || !far_tiles(box_gap2(tlo, thi, slo, shi), slo, shi, sg.near2);
+      if (!near) continue;  // block-uniform
+      any = true;
+      __syncthreads();  // the previous near tile is no longer read
+      stage_source(sg, ts + tid, w.s1, sp + tid, sv + tid, spl + tid, svl + tid);
+      wait_staged();
+      __syncthreads();
+      int skip[R];
+      Acc32 a[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        skip[r] = ti[r] - ts;
+        a[r] = Acc32{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      }
+      if (diag)
+        tile_near<DIFF, true, P, R, TB, KERN, NX>(sp, sv, spl, svl, g, skip, T, tpl, tvl, a);
+      else
+        tile_near<DIFF, false, P, R, TB, KERN, NX>(sp, sv, spl, svl, g, skip, T, tpl, tvl, a);
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        ou[r][0] += A * a[r].ux;
+        ou[r][1] += A * a[r].uy;
+        ou[r][2] += A * a[r].uz;
+        oa[r][0] += A * a[r].qx + 3.0 * A * a[r].gx;
+        oa[r][1] += A * a[r].qy + 3.0 * A * a[r].gy;
+        oa[r][2] += A * a[r].qz + 3.0 * A * a[r].gz;
+        if (DIFF) {
+          const double v = T[r].v;
+          oa[r][0] += cnu * (v * a[r].ex + (double)a[r].ev * ax[r]);
+          oa[r][1] += cnu * (v * a[r].ey + (double)a[r].ev * ay[r]);
+          oa[r][2] += cnu * (v * a[r].ez + (double)a[r].ev * az[r]);
+        }
+      }
+    }
+
+    const size_t fi = (size_t)(w.t0 / TPB) * (size_t)sg.nchunks + (size_t)w.chunk;
+    if (any) {
+      if (P > 1) {
+#pragma unroll
+        for (int off = 1; off < P; off <<= 1) {
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            ou[0][k] += __shfl_xor_sync(0xffffffffu, ou[0][k], off);
+            oa[0][k] += __shfl_xor_sync(0xffffffffu, oa[0][k], off);
+          }
+        }
+      }
+      if (g == 0) {
+        double *ns = sg.near_partial + fi * 6 * (size_t)TPB;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          if (!valid[r]) continue;
+          const int q = ti[r] - w.t0;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            ns[(size_t)k * TPB + q] = ou[r][k];
+            ns[(size_t)(3 + k) * TPB + q] = oa[r][k];
+          }
+        }
+      }
+    }
+    if (tid == 0) sg.near_flag[fi] = any ? 1 : 0;
+  }
+}
+
 using KernelFn = void (*)(const WorkItem *, int, const SegDesc *, int *);
 
+// The kernels of a tiling: the pair kernel (the far pass when split) and,
+// for split tilings, the near pass.
+struct Kernels {
+  KernelFn main = nullptr;
+  KernelFn near = nullptr;
+};
+
 template <bool DIFF>
-KernelFn select_highorder(const PairConfig &c) {
+Kernels select_highorder(const PairConfig &c) {
 #define PAWAN_F32_CASE_PK(TB_, P_, R_, U_, MINB_, PK_)                                   \
   PAWAN_F32_CASE_K(TB_, P_, R_, U_, MINB_, PK_, KERNEL_HIGHORDER)
+#define PAWAN_F32_MATCH(TB_, P_, R_, U_, MINB_, PK_)                                     \
+  (c.tb == TB_ && c.p == P_ && c.r == R_ && c.unroll == U_ && c.packed == PK_ &&         \
+   (c.minb == MINB_ || (c.minb == 0 && MINB_ == (TB_ <= 128 ? 4 : 2))))
 #define PAWAN_F32_CASE_K(TB_, P_, R_, U_, MINB_, PK_, KERN_)                             \
-  if (c.tb == TB_ && c.p == P_ && c.r == R_ && c.unroll == U_ && c.packed == PK_ &&      \
-      (c.minb == MINB_ || (c.minb == 0 && MINB_ == (TB_ <= 128 ? 4 : 2))))              \
-    return &pairs_f32_kernel<TB_, P_, R_, U_, DIFF, MINB_, PK_, KERN_>;
+  if (c.split == 0 && PAWAN_F32_MATCH(TB_, P_, R_, U_, MINB_, PK_))                       \
+    return Kernels{&pairs_f32_kernel<TB_, P_, R_, U_, DIFF, MINB_, PK_, KERN_>, nullptr};
+#define PAWAN_F32_CASE_SPLIT(TB_, U_, MINB_, PK_)                                        \
+  if (c.split == 1 && PAWAN_F32_MATCH(TB_, 1, 1, U_, MINB_, PK_))                         \
+    return Kernels{&pairs_f32_kernel<TB_, 1, 1, U_, DIFF, MINB_, PK_, KERNEL_HIGHORDER, true>, \
+                   &pairs_f32_near_kernel<TB_, 1, 1, DIFF, MINB_, KERNEL_HIGHORDER, 1>};
 #define PAWAN_F32_CASE(TB_, P_, R_, U_, MINB_) PAWAN_F32_CASE_PK(TB_, P_, R_, U_, MINB_, 0)
   PAWAN_F32_CASE_PK(128, 1, 1, 1, 4, 1)
   PAWAN_F32_CASE_PK(128, 1, 1, 2, 4, 1)
@@ -906,28 +1113,34 @@ KernelFn select_highorder(const PairConfig &c) {
   PAWAN_F32_CASE(256, 1, 2, 1, 2)
   PAWAN_F32_CASE(256, 1, 2, 2, 2)
   PAWAN_F32_CASE(256, 1, 1, 4, 3)
-  return nullptr;
+  PAWAN_F32_CASE_SPLIT(256, 4, 2, 1)
+  PAWAN_F32_CASE_SPLIT(256, 4, 2, 2)
+  PAWAN_F32_CASE_SPLIT(128, 4, 4, 1)
+  PAWAN_F32_CASE_SPLIT(128, 4, 4, 2)
+  return Kernels{};
 }
 
 // The Gaussian kernel is compiled for the default tilings only (packed mode 2:
 // its far tiles never take the uniform-radius branch that modes 1 and 2 differ in).
 template <bool DIFF>
-KernelFn select_gaussian(const PairConfig &c) {
+Kernels select_gaussian(const PairConfig &c) {
   PAWAN_F32_CASE_K(128, 1, 1, 4, 4, 2, KERNEL_GAUSSIAN)
   PAWAN_F32_CASE_K(128, 1, 1, 2, 4, 0, KERNEL_GAUSSIAN)
   PAWAN_F32_CASE_K(128, 2, 1, 4, 4, 0, KERNEL_GAUSSIAN)
   PAWAN_F32_CASE_K(256, 1, 1, 4, 2, 2, KERNEL_GAUSSIAN)
-  return nullptr;
+  return Kernels{};
 }
 #undef PAWAN_F32_CASE
 #undef PAWAN_F32_CASE_PK
 #undef PAWAN_F32_CASE_K
+#undef PAWAN_F32_CASE_SPLIT
+#undef PAWAN_F32_MATCH
 
-KernelFn select(const PairConfig &c, bool diffusion, int kernel) {
+Kernels select(const PairConfig &c, bool diffusion, int kernel) {
   if (kernel == KERNEL_GAUSSIAN) return diffusion ? select_gaussian<true>(c) : select_gaussian<false>(c);
   if (kernel == KERNEL_HIGHORDER)
     return diffusion ? select_highorder<true>(c) : select_highorder<false>(c);
-  return nullptr;
+  return Kernels{};
 }
 
 // Dynamic shared memory of a tiling: the staged ring plus the packed far format.
@@ -954,27 +1167,33 @@ cudaError_t prepare(KernelFn f, size_t bytes) {
 }  // namespace
 
 bool pairs_f32_supported(const PairConfig &c, int kernel) {
-  return select(c, true, kernel) != nullptr;
+  return select(c, true, kernel).main != nullptr;
 }
 
 cudaError_t pairs_f32_occupancy(const PairConfig &c, bool diffusion, int kernel, int *blocks_per_sm) {
-  KernelFn f = select(c, diffusion, kernel);
-  if (!f) return cudaErrorInvalidValue;
+  const Kernels k = select(c, diffusion, kernel);
+  if (!k.main) return cudaErrorInvalidValue;
   const size_t bytes = smem_bytes(c);
-  cudaError_t e = prepare(f, bytes);
+  cudaError_t e = prepare(k.main, bytes);
   if (e != cudaSuccess) return e;
-  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, f, c.tb, bytes);
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, k.main, c.tb, bytes);
 }
 
 cudaError_t launch_pairs_f32(const PairConfig &c, bool diffusion, int kernel, int grid,
                              const WorkItem *items, int n_items, const SegDesc *segs,
                              int *next_item, cudaStream_t s) {
-  KernelFn f = select(c, diffusion, kernel);
-  if (!f) return cudaErrorInvalidValue;
+  const Kernels k = select(c, diffusion, kernel);
+  if (!k.main) return cudaErrorInvalidValue;
   const size_t bytes = smem_bytes(c);
-  cudaError_t e = prepare(f, bytes);
+  cudaError_t e = prepare(k.main, bytes);
   if (e != cudaSuccess) return e;
-  f<<<grid, c.tb, bytes, s>>>(items, n_items, segs, next_item);
+  if (k.near) {
+    // the near pass first (static shared memory only), on the second counter
+    k.near<<<grid, c.tb, 0, s>>>(items, n_items, segs, next_item + 1);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  k.main<<<grid, c.tb, bytes, s>>>(items, n_items, segs, next_item);
   return cudaGetLastError();
 }
 

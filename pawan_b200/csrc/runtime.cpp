@@ -60,6 +60,14 @@ std::vector<TileChoice> tile_candidates(int precision, int kernel) {
         t.pc = PairConfig{tb, sh[0], sh[2], sh[1], sh[3], sh[4]};
         if (pairs_f32_supported(t.pc, kernel)) v.push_back(t);
       }
+    // the packed unroll-4 shapes again with a separate near pass (ahead where
+    // near tile pairs are many: ragged batches of small rings, scrambled states)
+    for (int tb : {128, 256})
+      for (int pk : {1, 2}) {
+        TileChoice t;
+        t.pc = PairConfig{tb, 1, 4, 1, 0, pk, 1};
+        if (pairs_f32_supported(t.pc, kernel)) v.push_back(t);
+      }
   } else {
     for (int tb : {128, 256}) {
       TileChoice t;
@@ -159,8 +167,8 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
   // per system: partial slots [target tiles][chunks][6][TPB] (none with one
   // chunk), rates [6][n], one counter per target tile
   if (TPB % 8 != 0) return fail(ctx, PAWAN_ERR_INVALID, "targets per block must be a multiple of 8");
-  size_t partial_total = 0, box_total = 0, rates_total = 0, count_total = 0;
-  std::vector<size_t> partial_off(systems.size()), box_off(systems.size());
+  size_t partial_total = 0, box_total = 0, rates_total = 0, count_total = 0, slot_total = 0;
+  std::vector<size_t> partial_off(systems.size()), box_off(systems.size()), slot_off(systems.size());
   std::vector<size_t> rates_off(systems.size()), count_off(systems.size());
   std::vector<double> sys_cost(systems.size(), 0.0);
   p->nchunks.resize(systems.size());
@@ -176,6 +184,8 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     const size_t target_tiles = ((size_t)n + TPB - 1) / TPB;
     partial_off[s] = partial_total;
     if (nch > 1) partial_total += target_tiles * (size_t)nch * 6 * (size_t)TPB;
+    slot_off[s] = slot_total;  // item slots (target tile, chunk), for the near pass
+    slot_total += target_tiles * (size_t)nch;
     rates_off[s] = rates_total;
     rates_total += 6 * (size_t)n;
     count_off[s] = count_total;
@@ -213,6 +223,8 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     p->partial.ordered_on(ctx->stream);
     p->rates.ordered_on(ctx->stream);
     p->tile_count.ordered_on(ctx->stream);
+    p->near_partial.ordered_on(ctx->stream);
+    p->near_flag.ordered_on(ctx->stream);
     p->boxes.ordered_on(ctx->stream);
     p->items.ordered_on(ctx->stream);
     p->segs.ordered_on(ctx->stream);
@@ -228,6 +240,10 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
   PAWAN_CUDA(ctx, p->rates.alloc(rates_total));
   PAWAN_CUDA(ctx, p->tile_count.alloc(count_total));
   PAWAN_CUDA(ctx, cudaMemsetAsync(p->tile_count.p, 0, p->tile_count.bytes(), ctx->stream));
+  if (tile.pc.split > 0) {
+    PAWAN_CUDA(ctx, p->near_partial.alloc(slot_total * 6 * (size_t)TPB));
+    PAWAN_CUDA(ctx, p->near_flag.alloc(slot_total));
+  }
   PAWAN_CUDA(ctx, p->boxes.alloc(box_total));
   std::vector<WorkItem> wh(items.size());
   p->item_costs.resize(items.size());
@@ -251,6 +267,8 @@ int build_plan(pawan_ctx *ctx, const std::vector<pawan_system *> &systems, int p
     d.partial = p->nchunks[s] > 1 ? p->partial.p + partial_off[s] : nullptr;
     d.rates = p->rates.p + rates_off[s];
     d.tile_count = p->tile_count.p + count_off[s];
+    d.near_partial = tile.pc.split > 0 ? p->near_partial.p + slot_off[s] * 6 * (size_t)TPB : nullptr;
+    d.near_flag = tile.pc.split > 0 ? p->near_flag.p + slot_off[s] : nullptr;
     d.n = (int)y->n;
     d.nchunks = p->nchunks[s];
     d.nu = y->nu;
@@ -363,7 +381,7 @@ int launch_pairs_range(pawan_ctx *ctx, Plan &p, int first, int count, bool allow
       PAWAN_TRY(launch_stage_mode(ctx, p, STAGE_PACK));
       break;
     }
-  PAWAN_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(int), ctx->stream));
+  PAWAN_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, 2 * sizeof(int), ctx->stream));
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (ctx->profile && allow_events) {
     e0 = take_event(ctx);

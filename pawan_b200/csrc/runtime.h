@@ -67,7 +67,7 @@ struct TileChoice {
   int items_per_slot = 16;
   bool operator==(const TileChoice &o) const {
     return pc.tb == o.pc.tb && pc.p == o.pc.p && pc.r == o.pc.r && pc.unroll == o.pc.unroll &&
-           pc.minb == o.pc.minb && pc.packed == o.pc.packed &&
+           pc.minb == o.pc.minb && pc.packed == o.pc.packed && pc.split == o.pc.split &&
            items_per_slot == o.items_per_slot;
   }
 };
@@ -169,6 +169,8 @@ struct Plan {
   DBuf<double> partial;   // per system [target tiles][chunks][6][tpb] (chunks > 1)
   DBuf<double> rates;     // per system [6][n]: the summed chunks
   DBuf<int> tile_count;   // per system and target tile; 0 between launches
+  DBuf<double> near_partial;        // split tilings: near sums per item slot (as partial)
+  DBuf<unsigned char> near_flag;    // split tilings: per item slot, whether it had near tiles
   DBuf<float4> boxes;
   DBuf<WorkItem> items;
   DBuf<SegDesc> segs;

@@ -60,7 +60,8 @@ def test_tile_candidates_listed_host_side():
     """The autotuner's candidate tilings and chunkings, without a GPU; the
     full-size parity tests (tests/test_gpu_pairs.py) run exactly these."""
     from test_gpu_pairs import DEFAULT_TILING, TIMED_TILING, TUNE_CANDIDATES
-    keys = ("threads", "threads_per_target", "targets_per_thread", "unroll", "blocks_per_sm", "packed")
+    keys = ("threads", "threads_per_target", "targets_per_thread", "unroll", "blocks_per_sm", "packed",
+            "split_near")
     got = [tuple(c[k] for k in keys) for c in pawan_b200.tile_candidates("f32")]
     assert got == TUNE_CANDIDATES
     assert TIMED_TILING in got and DEFAULT_TILING in got

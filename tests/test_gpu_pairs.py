@@ -260,15 +260,17 @@ def test_invalid_arguments_raise(ctx):
 # The tilings the autotuner times (pawan_tile_candidates; tests/test_abi.py
 # checks this list against the library's): (threads, threads per target,
 # targets per thread, unroll, blocks per SM, packed mode).
-TUNE_CANDIDATES = [(tb,) + sh for tb in (128, 256) for sh in (
+TUNE_CANDIDATES = [(tb,) + sh + (0,) for tb in (128, 256) for sh in (
     (1, 1, 4, 0, 0), (2, 1, 4, 0, 0), (4, 1, 4, 0, 0), (1, 2, 1, 0, 0), (1, 2, 2, 0, 0),
     (1, 1, 4, 5, 0), (1, 1, 1, 0, 1), (1, 1, 2, 0, 1), (1, 1, 4, 0, 1), (1, 1, 2, 5, 1),
     (1, 1, 2, 0, 2), (1, 1, 4, 0, 2))
     if not (tb == 256 and sh in ((1, 1, 4, 5, 0), (1, 1, 1, 0, 1), (1, 1, 2, 5, 1)))]
+# ... and with a separate near pass (the last field)
+TUNE_CANDIDATES += [(tb, 1, 1, 4, 0, pk, 1) for tb in (128, 256) for pk in (1, 2)]
 # the tiling the default bench run's autotuner picks on the ring pair, and the
 # library's default tiling
-TIMED_TILING = (256, 1, 1, 4, 0, 1)
-DEFAULT_TILING = (128, 1, 1, 4, 0, 2)
+TIMED_TILING = (256, 1, 1, 4, 0, 1, 0)
+DEFAULT_TILING = (128, 1, 1, 4, 0, 2, 0)
 FULL_SAMPLES = 4096
 
 
@@ -293,8 +295,9 @@ def full(ctx):
 
 def _check_full(full, name, tiling, ips):
     s, t, (u_ref, da_ref) = full(name)
-    tb, p, r, unroll, minb, mode = tiling
-    s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=mode)
+    tb, p, r, unroll, minb, mode, split = tiling
+    s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=mode,
+                 split_near=split)
     s.solve()
     u, da = s.union_rates()
     check("f32", u[t], da[t], u_ref, da_ref)
@@ -372,8 +375,10 @@ def test_tile_classes_at_their_boundaries(ctx, gap, mixed):
             (cfg, rms_rel(du, du_ref), rms_rel(dda, dda_ref))
 
 
-@pytest.mark.parametrize("tiling", [TIMED_TILING, DEFAULT_TILING, (128, 2, 1, 4, 0, 0), (128, 1, 2, 2, 0, 0)],
-                         ids=["timed", "default", "two-threads-per-target", "two-targets-per-thread"])
+@pytest.mark.parametrize("tiling", [TIMED_TILING, DEFAULT_TILING, (128, 2, 1, 4, 0, 0, 0), (128, 1, 2, 2, 0, 0, 0),
+                                    (256, 1, 1, 4, 0, 1, 1)],
+                         ids=["timed", "default", "two-threads-per-target", "two-targets-per-thread",
+                              "near-pass"])
 def test_chunk_sums_inside_the_launch(ctx, tiling):
     """The pair kernels sum a target tile's chunk partials inside the launch
     (the block completing the tile, in chunk order).  With the tiling fixed,
@@ -385,11 +390,12 @@ def test_chunk_sums_inside_the_launch(ctx, tiling):
     ragged last tile.  (A single chunk, where items write the rates directly,
     is the small systems of test_ragged_sizes_against_restatement.)"""
     sc = g.ring_pair(n_stations=300, seed=61, nu=1e-4)  # N = 4,800: ragged target tiles
-    tb, p, r, unroll, minb, mode = tiling
+    tb, p, r, unroll, minb, mode, split = tiling
     s = System.from_scenario(ctx, sc, "f32")
     results = []
     for ips in (1, 2, 8, 32, 128, 1024):
-        s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=mode)
+        s.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=mode,
+                     split_near=split)
         s.solve()
         first = s.union_rates()
         s.solve()
