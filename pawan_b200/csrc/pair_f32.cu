@@ -54,6 +54,10 @@
 //    >= 6 sigma_max): the far formulation without the Z terms, which are below
 //    3e-9 of the terms they are added to there (kernel_scalars_nz); 29 FP32
 //    instructions per pair with one radius, no diffusion sums.
+//  * far tiles whose every pair is at least 16 smoothing radii apart: the
+//    Z-free field with its smoothing factor by a two-term series exact to
+//    3e-8 there (kernel_scalars_series); one MUFU rsqrt per pair instead of
+//    an rsqrt and a reciprocal.
 // After each tile both are folded into six FP64 sums (u, dalpha) with the
 // target's strength in FP64 (hi + lo).
 //
@@ -191,6 +195,25 @@ __device__ __forceinline__ void kernel_scalars_nz(float sig2, float r2, float &q
   nfh = qh * ri2;
 }
 
+// Far field without the Z terms, and a series for the smoothing factor.
+// With eps = sigma^2 / rho^2,
+//   rho^2 y (1 + y sigma^2/2) = 1/(1 + eps) + (eps/2)/(1 + eps)^2
+//                             = 1 - eps/2 + 0 eps^2 + eps^3/2 - ...,
+// so where every pair of a tile pair has rho >= 16 sigma (eps <= 1/256, checked
+// on the tiles' boxes) the two-term form 1 - sigma^2/(2 rho^2) is exact to
+// 3.0e-8 relative, below FP32's unit roundoff (6e-8):
+//   qh = sigma^2 rho^-5 (1 - sigma^2 rho^-2 / 2),   fh = -qh / rho^2,
+// one MUFU rsqrt per pair instead of an rsqrt and a reciprocal (the
+// uniform-radius form returns qs = qh / sigma^2 = rho^-5 (1 - h rho^-2)).
+__device__ __forceinline__ void kernel_scalars_series(float sig2, float r2, float &qh, float &nfh) {
+  const float ri = rsqrtf(r2);
+  const float ri2 = ri * ri;
+  const float e = sig2 * ri2;
+  const float c = fmaf(-0.5f, e, 1.0f);
+  qh = e * ri * ri2 * c;
+  nfh = qh * ri2;
+}
+
 // The Gaussian kernel (gaussian.h:20-59) in the units of kernel_scalars: with
 // x2 = rho^2/sigma^2, e = exp(-x2/2) and K = sqrt(2/pi),
 //   qh = gq / sigma^3,        gq = (erf(x/sqrt 2)/x - K e) / x2,
@@ -246,8 +269,9 @@ __device__ __forceinline__ void gauss_scalars(float sig2, float r2, float ri, fl
 // Far tile, shared-memory format (written when the tile is staged):
 //   sa[j] = (x'_j, h_j),  sb[j] = (alpha_j, v_j),  sc[j] = (beta_j, 0).
 // UNI: every pair has sigma^2 = 2 hu (sums in the units of
-// kernel_scalars_uniform).
-template <bool DIFF, bool UNI, int P, int R, int NSRC, int U, int KERN, bool NZ>
+// kernel_scalars_uniform).  NZ: the Z-free far field; SER (with NZ): its
+// two-term series (kernel_scalars_series).
+template <bool DIFF, bool UNI, int P, int R, int NSRC, int U, int KERN, bool NZ, bool SER = false>
 __device__ __forceinline__ void tile_far(const float4 *__restrict__ sa,
                                          const float4 *__restrict__ sb,
                                          const float4 *__restrict__ sc, int g,
@@ -266,7 +290,20 @@ __device__ __forceinline__ void tile_far(const float4 *__restrict__ sa,
       const float dx = F[r].x - p.x, dy = F[r].y - p.y, dz = F[r].z - p.z;
       const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
       float qh, fh, dp;
-      if (NZ) {
+      if (NZ && SER) {
+        // Z-free far field by the series (kernel_scalars_series)
+        float nfh;
+        if (UNI) {
+          const float ri = rsqrtf(r2);
+          const float ri2 = ri * ri;
+          qh = ri * ri2 * fmaf(-hu, ri2, 1.0f) * ri2;
+          nfh = qh * ri2;
+        } else {
+          kernel_scalars_series(T[r].h + p.w, r2, qh, nfh);
+        }
+        fh = -nfh;
+        dp = 0.f;
+      } else if (NZ) {
         // Z-free far field (kernel_scalars_nz); the diffusion sums stay 0
         float nfh;
         if (UNI) {
@@ -356,7 +393,7 @@ __device__ __forceinline__ float2 inv_r2(float2 r2, float2 ri) {
   return __fmul2_rn(ri, ri);
 }
 
-template <bool DIFF, bool UNI, int RM, int NSRC, int U, int KERN, bool NZ>
+template <bool DIFF, bool UNI, int RM, int NSRC, int U, int KERN, bool NZ, bool SER = false>
 __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
                                                 const float4 *__restrict__ f1,
                                                 const float4 *__restrict__ f2,
@@ -365,6 +402,7 @@ __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
                                                 const float2 *__restrict__ f5, const Target2 &T,
                                                 float hu, Acc2 &a) {
   const float2 s2u = bc2(2.f * hu), h2 = bc2(hu), c240 = bc2(-480.f * hu);
+  const float2 nh2 = bc2(-hu), one2 = bc2(1.0f), nhalf2 = bc2(-0.5f);
 #pragma unroll U
   for (int k = 0; k < NSRC / 2; ++k) {
     const float4 A0 = f0[k], A1 = f1[k], A2 = f2[k], A3 = f3[k], A4 = f4[k];
@@ -379,7 +417,21 @@ __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
     const float2 dz = __fadd2_rn(T.z, npz);
     const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
     float2 qh, nfh, dp;
-    if (NZ) {
+    if (NZ && SER) {
+      // Z-free far field by the series in pairs (kernel_scalars_series):
+      // one MUFU rsqrt per source (and a reciprocal for 1/rho^2 when RM =
+      // 1), 5 FP32x2 operations with one radius (6 when RM = 2)
+      const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+      const float2 ri2 = inv_r2<RM>(r2, ri);
+      if (UNI) {
+        qh = __fmul2_rn(__fmul2_rn(__fmul2_rn(ri, ri2), __ffma2_rn(nh2, ri2, one2)), ri2);
+      } else {
+        const float2 e = __fmul2_rn(__fadd2_rn(T.h, hj), ri2);
+        qh = __fmul2_rn(__fmul2_rn(__fmul2_rn(e, ri), ri2), __ffma2_rn(nhalf2, e, one2));
+      }
+      nfh = __fmul2_rn(qh, ri2);
+      dp = make_float2(0.f, 0.f);
+    } else if (NZ) {
       // Z-free far field in pairs (kernel_scalars_nz), no diffusion sums
       if (UNI) {
         const float2 sr = __fadd2_rn(r2, s2u);
@@ -702,6 +754,8 @@ __global__ void __launch_bounds__(TB, MINB)
       // every pair at rho >= 6 sigma: the Z-free far field (w of a box = the
       // range of h = s^2/2, so thi.w + shi.w is the largest sigma^2)
       const bool nz = KERN == KERNEL_HIGHORDER && !near && gap2 >= 36.f * (thi.w + shi.w);
+      // every pair at rho >= 16 sigma: the Z-free field by its series
+      const bool ser = nz && gap2 >= 256.f * (thi.w + shi.w);
       // one smoothing radius over both tiles
       const bool uni = KERN == KERNEL_HIGHORDER && tlo.w == thi.w && slo.w == shi.w && tlo.w == slo.w;
       const float cx = 0.5f * (slo.x + shi.x), cy = 0.5f * (slo.y + shi.y),
@@ -772,7 +826,11 @@ __global__ void __launch_bounds__(TB, MINB)
         const float4 *f0 = fq + buf * FQ, *f1 = fq + (2 + buf) * FQ, *f2 = fq + (4 + buf) * FQ,
                      *f3 = fq + (6 + buf) * FQ, *f4 = fq + (8 + buf) * FQ;
         const float2 *f5 = fz + buf * FQ;
-        if (nz && uni)
+        if (ser && uni)
+          tile_far_packed<DIFF, true, PK, TB, U, KERN, true, true>(f0, f1, f2, f3, f4, f5, T2, slo.w, b);
+        else if (ser)
+          tile_far_packed<DIFF, false, PK, TB, U, KERN, true, true>(f0, f1, f2, f3, f4, f5, T2, 0.f, b);
+        else if (nz && uni)
           tile_far_packed<DIFF, true, PK, TB, U, KERN, true>(f0, f1, f2, f3, f4, f5, T2, slo.w, b);
         else if (nz)
           tile_far_packed<DIFF, false, PK, TB, U, KERN, true>(f0, f1, f2, f3, f4, f5, T2, 0.f, b);
@@ -810,7 +868,11 @@ __global__ void __launch_bounds__(TB, MINB)
           F[r].gz = fmaf(F[r].x, T[r].bh, -F[r].y * T[r].ah);
         }
         const float4 *ta = sp + buf * TB, *tb = sv + buf * TB, *tc = spl + buf * TB;
-        if (nz && uni)
+        if (ser && uni)
+          tile_far<DIFF, true, P, R, TB, U, KERN, true, true>(ta, tb, tc, g, T, F, slo.w, a);
+        else if (ser)
+          tile_far<DIFF, false, P, R, TB, U, KERN, true, true>(ta, tb, tc, g, T, F, 0.f, a);
+        else if (nz && uni)
           tile_far<DIFF, true, P, R, TB, U, KERN, true>(ta, tb, tc, g, T, F, slo.w, a);
         else if (nz)
           tile_far<DIFF, false, P, R, TB, U, KERN, true>(ta, tb, tc, g, T, F, 0.f, a);

@@ -325,11 +325,13 @@ def test_full_size_timed_tiling_every_chunking(full, name, tiling, ips):
 
 
 @pytest.mark.parametrize("mixed", [False, True])
-@pytest.mark.parametrize("gap", [3.0, 4.5, 5.5, 6.5, 10.0])
+@pytest.mark.parametrize("gap", [3.0, 4.5, 5.5, 6.5, 10.0, 15.0, 17.0, 20.0])
 def test_tile_classes_at_their_boundaries(ctx, gap, mixed):
     """Two compact clusters of 256 particles (two 128-tiles each) whose boxes
     are `gap` smoothing radii apart: near (< 4 s), far with the Z terms
-    (4 s .. 6 s) and far without them (>= 6 s, where Z is below 3e-9 of q).
+    (4 s .. 6 s), far without them (>= 6 s, where Z is below 3e-9 of q) and
+    far without them by the two-term series of the smoothing factor (>= 16 s,
+    truncation below 3e-8).
     The whole solve against the FP64 oracle; then the cross-cluster part at
     cluster A on its own, by linearity: the same system solved with cluster
     B's strengths doubled, minus the first solve, is at A exactly the part of
@@ -337,7 +339,7 @@ def test_tile_classes_at_their_boundaries(ctx, gap, mixed):
     both solves), compared with the same difference in the oracle.  nu != 0;
     packed and scalar tilings; one smoothing radius (the uniform-radius
     forms) or radii in [0.8 s, 1.2 s] (the general forms; the Z-free class
-    then starts at 7.2 s)."""
+    then starts at 7.2 s and the series at 19.2 s)."""
     rng = np.random.default_rng(int(gap * 10))
     s = 0.05
     n = 256
@@ -346,6 +348,15 @@ def test_tile_classes_at_their_boundaries(ctx, gap, mixed):
     b[:, 0] += (gap + 1.0) * s  # box gap = gap * s
     pos = np.concatenate([a, b])
     vor = rng.normal(size=(2 * n, 3)) * 1e-3
+    tol = 1e-5
+    if gap >= 15.0:
+        # from about 15 s on, the stretching that random strengths of a
+        # distant cluster drive cancels to a small fraction of its terms (the
+        # FP64-vs-FP32 distance of the exact Z-free form reaches 1.3e-5 at
+        # 17 s); a common strength direction keeps it well conditioned, so a
+        # tighter bound applies
+        vor[n:] += np.array([1e-3, 2e-3, -1.5e-3])
+        tol = 2e-6
     vor2 = vor.copy()
     vor2[n:] *= 2.0
     rad = s * rng.uniform(0.8, 1.2, 2 * n) if mixed else np.full(2 * n, s)
@@ -371,7 +382,7 @@ def test_tile_classes_at_their_boundaries(ctx, gap, mixed):
         sysm.solve()
         ug2, dag2 = sysm.union_rates()
         du, dda = (ug2 - ug1)[:n], (dag2 - dag1)[:n]
-        assert rms_rel(du, du_ref) < 1e-5 and rms_rel(dda, dda_ref) < 1e-5, \
+        assert rms_rel(du, du_ref) < tol and rms_rel(dda, dda_ref) < tol, \
             (cfg, rms_rel(du, du_ref), rms_rel(dda, dda_ref))
 
 
