@@ -558,14 +558,18 @@ __device__ __forceinline__ void projection_cross(float ax, float ay, float az, f
 // Near tile, shared-memory format: sp, sv, spl, svl = pos32, vor32, poslo,
 // vorlo of the sources; tpl, tvl = poslo, vorlo of the targets.
 // NX: alpha_i x alpha_j by cross_accurate (0) or projection_cross (1).
-template <bool DIFF, bool CHECK, int P, int R, int NSRC, int KERN, int NX = 0>
+// UNI: every pair has sigma^2 = 2 hu; the sums are then in the units of
+// kernel_scalars_uniform (qh, fh over sigma^2, Dp over 32).
+template <bool DIFF, bool CHECK, int P, int R, int NSRC, int KERN, int NX = 0, int NU = 1,
+          bool UNI = false>
 __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
                                           const float4 *__restrict__ sv,
                                           const float4 *__restrict__ spl,
                                           const float4 *__restrict__ svl, int g,
                                           const int (&skip)[R], const Target (&T)[R],
                                           const float4 (&tpl)[R], const float4 (&tvl)[R],
-                                          Acc32 (&a)[R]) {
+                                          Acc32 (&a)[R], float hu = 0.f) {
+  const float s2u = 2.f * hu, c240 = -480.f * hu;
   float iaa[R], lcx[R], lcy[R], lcz[R];  // per target, for projection_cross
   if (NX) {
 #pragma unroll
@@ -577,9 +581,10 @@ __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
       lcz[r] = fmaf(tvl[r].x, T[r].bh, -tvl[r].y * T[r].ah);
     }
   }
-  // near tiles are a few percent of the work: no unrolling keeps the register
-  // budget of the far loop
-#pragma unroll 1
+  // near tiles are a few percent of the work: inside the pair kernel no
+  // unrolling (NU = 1) keeps the register budget of the far loop; the separate
+  // near pass has its own and unrolls
+#pragma unroll NU
   for (int k = 0; k < NSRC / P; ++k) {
     const int jj = g + P * k;
     const float4 p = sp[jj];
@@ -597,6 +602,9 @@ __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
       float qh, fh, dp;
       if (KERN == KERNEL_GAUSSIAN) {
         gauss_scalars(sig2, r2, ri, qh, fh, dp);
+      } else if (UNI) {
+        const float w = rsqrtf(r2 + s2u);
+        kernel_scalars_uniform(hu, c240, w, ri, r2, qh, fh, dp);
       } else {
         const float w = rsqrtf(r2 + sig2);
         kernel_scalars(sig2, w, ri, qh, fh, dp);
@@ -984,7 +992,7 @@ __global__ void __launch_bounds__(TB, MINB)
 // with the accurate near formulation; an item's sums go to its near slot and
 // its flag says whether it had any.  It runs before the far pass, which adds
 // the flagged slots to its own sums.
-template <int TB, int P, int R, bool DIFF, int MINB, int KERN, int NX>
+template <int TB, int P, int R, bool DIFF, int MINB, int KERN, int NX, int NU = 2>
 __global__ void __launch_bounds__(TB, MINB)
     pairs_f32_near_kernel(const WorkItem *__restrict__ items, int n_items,
                           const SegDesc *__restrict__ segs, int *__restrict__ next_item) {
@@ -1067,23 +1075,34 @@ __global__ void __launch_bounds__(TB, MINB)
         skip[r] = ti[r] - ts;
         a[r] = Acc32{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       }
-      if (diag)
-        tile_near<DIFF, true, P, R, TB, KERN, NX>(sp, sv, spl, svl, g, skip, T, tpl, tvl, a);
+      // one smoothing radius over both tiles: the uniform-radius scalars
+      const bool uni = KERN == KERNEL_HIGHORDER && tlo.w == thi.w && slo.w == shi.w && tlo.w == slo.w;
+      if (diag && uni)
+        tile_near<DIFF, true, P, R, TB, KERN, NX, NU, true>(sp, sv, spl, svl, g, skip, T, tpl, tvl, a,
+                                                            slo.w);
+      else if (diag)
+        tile_near<DIFF, true, P, R, TB, KERN, NX, NU>(sp, sv, spl, svl, g, skip, T, tpl, tvl, a);
+      else if (uni)
+        tile_near<DIFF, false, P, R, TB, KERN, NX, NU, true>(sp, sv, spl, svl, g, skip, T, tpl, tvl,
+                                                             a, slo.w);
       else
-        tile_near<DIFF, false, P, R, TB, KERN, NX>(sp, sv, spl, svl, g, skip, T, tpl, tvl, a);
+        tile_near<DIFF, false, P, R, TB, KERN, NX, NU>(sp, sv, spl, svl, g, skip, T, tpl, tvl, a);
+      // undo the uniform-radius scaling: qh = sigma^2 qs, fh = sigma^2 fs, Dp = 32 ds
+      const double As2 = uni ? A * 2.0 * (double)slo.w : A;
+      const double cd = uni ? 32.0 * cnu : cnu;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
-        ou[r][0] += A * a[r].ux;
-        ou[r][1] += A * a[r].uy;
-        ou[r][2] += A * a[r].uz;
-        oa[r][0] += A * a[r].qx + 3.0 * A * a[r].gx;
-        oa[r][1] += A * a[r].qy + 3.0 * A * a[r].gy;
-        oa[r][2] += A * a[r].qz + 3.0 * A * a[r].gz;
+        ou[r][0] += As2 * a[r].ux;
+        ou[r][1] += As2 * a[r].uy;
+        ou[r][2] += As2 * a[r].uz;
+        oa[r][0] += As2 * a[r].qx + 3.0 * As2 * a[r].gx;
+        oa[r][1] += As2 * a[r].qy + 3.0 * As2 * a[r].gy;
+        oa[r][2] += As2 * a[r].qz + 3.0 * As2 * a[r].gz;
         if (DIFF) {
           const double v = T[r].v;
-          oa[r][0] += cnu * (v * a[r].ex + (double)a[r].ev * ax[r]);
-          oa[r][1] += cnu * (v * a[r].ey + (double)a[r].ev * ay[r]);
-          oa[r][2] += cnu * (v * a[r].ez + (double)a[r].ev * az[r]);
+          oa[r][0] += cd * (v * a[r].ex + (double)a[r].ev * ax[r]);
+          oa[r][1] += cd * (v * a[r].ey + (double)a[r].ev * ay[r]);
+          oa[r][2] += cd * (v * a[r].ez + (double)a[r].ev * az[r]);
         }
       }
     }
