@@ -57,8 +57,9 @@ typedef struct {
                              squared; 0: one source per instruction */
   int split_near;         /* FP32: 1 computes the near tile pairs in a pass of
                              their own before the far pass (each kernel with its
-                             own registers; faster where near pairs are many);
-                             0: one pass */
+                             own registers; faster where near pairs are many),
+                             2 the same with the near pass two sources per
+                             FP32x2 instruction; 0: one pass */
 } pawan_tiling;
 
 typedef struct pawan_ctx pawan_ctx;

@@ -17,7 +17,8 @@ namespace pawan {
 // `split` = 1: near tile pairs are computed by a pass of their own before the
 // far pass (which then skips them), each kernel with its own register
 // allocation, the near pass forming alpha_i x alpha_j by the projection form
-// (19 operations instead of the one pass's 27).
+// (19 operations instead of the one pass's 27); `split` = 2: the same with the
+// near pass two sources per FP32x2 instruction.
 struct PairConfig {
   int tb;
   int p;

@@ -652,6 +652,143 @@ __device__ __forceinline__ void tile_near(const float4 *__restrict__ sp,
   }
 }
 
+// ---- packed near tiles: two sources per FP32x2 instruction ----------------
+// tile_near's arithmetic (hi/lo differences, the projection cross product)
+// on a pair of sources per instruction, for the separate near pass, whose
+// scalar loop is bound by instruction issue.  Shared-memory layout of a near
+// tile, per source pair k = (a, b) = (2k, 2k+1):
+//   n0[k] = (-xh_a, -xh_b, -yh_a, -yh_b)   n1[k] = (-zh_a, -zh_b, h_a, h_b)
+//   n2[k] = (-xl_a, -xl_b, -yl_a, -yl_b)   n3[k] = (-zl_a, -zl_b, -v_a, -v_b)
+//   n4[k] = (ax_a, ax_b, ay_a, ay_b)       n5[k] = (az_a, az_b, axl_a, axl_b)
+//   n6[k] = (ayl_a, ayl_b, azl_a, azl_b)   n7[k] = (-ax_a, -ax_b, -ay_a, -ay_b)
+//   n8[k] = (-az_a, -az_b)
+// (h = s/2 squared, x hi/lo, alpha hi/lo, v the volume).  Positions, the
+// volume and a second copy of the strength are stored negated so that no
+// operand is negated in the loop; the target's quantities enter as broadcast
+// pairs.  The loop accumulates -fh (as the packed far loop does).
+struct NearT2 {
+  float2 xh, yh, zh, xl, yl, zl;  // position hi, lo
+  float2 h;                       // h_i
+  float2 ax, ay, az;              // strength hi
+  float2 nax, nay, naz;           // -strength hi
+  float2 nlx, nly, nlz;           // -(alpha_lo x alpha_hi) of the target
+  float2 iaa;                     // 1 / |alpha_hi|^2 (0 for alpha = 0)
+  float2 nalx, naly, nalz;        // -strength lo
+  float2 v;                       // volume
+};
+
+struct NearAcc2 {
+  float2 ux, uy, uz;  // sum qh (alpha_j x d)
+  float2 qx, qy, qz;  // sum qh (alpha_i x alpha_j)
+  float2 gx, gy, gz;  // sum -fh t d
+  float2 ex, ey, ez;  // sum Dp delta
+  float2 ev;          // sum Dp (v_i - v_j)
+};
+
+// CHECK: the tile holds the target (skip = its index in the tile, whose pair
+// contributes nothing).  UNI: every pair has sigma^2 = 2 hu (the sums in the
+// units of kernel_scalars_uniform).
+template <bool DIFF, bool CHECK, bool UNI, int RM, int NSRC>
+__device__ __forceinline__ void tile_near_packed(const float4 *__restrict__ n0,
+                                                 const float4 *__restrict__ n1,
+                                                 const float4 *__restrict__ n2,
+                                                 const float4 *__restrict__ n3,
+                                                 const float4 *__restrict__ n4,
+                                                 const float4 *__restrict__ n5,
+                                                 const float4 *__restrict__ n6,
+                                                 const float4 *__restrict__ n7,
+                                                 const float2 *__restrict__ n8, int skip,
+                                                 const NearT2 &T, float hu, NearAcc2 &a) {
+  const float2 s2u = bc2(2.f * hu), h2 = bc2(hu), c240 = bc2(-480.f * hu);
+#pragma unroll 1
+  for (int k = 0; k < NSRC / 2; ++k) {
+    const float4 A0 = n0[k], A1 = n1[k], A2 = n2[k], A3 = n3[k];
+    const float2 dx = __fadd2_rn(__fadd2_rn(T.xh, make_float2(A0.x, A0.y)),
+                                 __fadd2_rn(T.xl, make_float2(A2.x, A2.y)));
+    const float2 dy = __fadd2_rn(__fadd2_rn(T.yh, make_float2(A0.z, A0.w)),
+                                 __fadd2_rn(T.yl, make_float2(A2.z, A2.w)));
+    const float2 dz = __fadd2_rn(__fadd2_rn(T.zh, make_float2(A1.x, A1.y)),
+                                 __fadd2_rn(T.zl, make_float2(A3.x, A3.y)));
+    const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+    const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    float2 qh, nfh, dp;
+    if (UNI) {
+      // kernel_scalars_uniform in pairs, returning -fs
+      const float2 sr = __fadd2_rn(r2, s2u);
+      const float2 w = make_float2(rsqrtf(sr.x), rsqrtf(sr.y));
+      const float2 ri2 = inv_r2<RM>(r2, ri);
+      const float2 y = __fmul2_rn(w, w);
+      const float2 u = __fmul2_rn(h2, y);
+      const float2 v = __fmul2_rn(u, w);
+      const float2 v2 = __fmul2_rn(v, v);
+      dp = __fmul2_rn(__fmul2_rn(v2, v2), v);
+      const float2 ph = __fmul2_rn(__ffma2_rn(u, y, y), ri);
+      qh = __fmul2_rn(__ffma2_rn(c240, dp, ph), ri2);
+      nfh = __fmul2_rn(__ffma2_rn(bc2(-80.f), dp, qh), ri2);
+    } else {
+      // kernel_scalars in pairs, returning -fh
+      const float2 sig2 = __fadd2_rn(T.h, make_float2(A1.z, A1.w));
+      const float2 sr = __fadd2_rn(r2, sig2);
+      const float2 w = make_float2(rsqrtf(sr.x), rsqrtf(sr.y));
+      const float2 w2 = __fmul2_rn(w, w);
+      const float2 uu = __fmul2_rn(sig2, w2);
+      const float2 v = __fmul2_rn(uu, w);
+      const float2 v2 = __fmul2_rn(v, v);
+      dp = __fmul2_rn(__fmul2_rn(v2, v2), v);
+      const float2 zc = __fmul2_rn(dp, sig2);
+      const float2 ph = __fmul2_rn(__fmul2_rn(__ffma2_rn(bc2(0.5f), uu, bc2(1.0f)), w2), ri);
+      const float2 ri2 = __fmul2_rn(ri, ri);
+      qh = __fmul2_rn(__fmul2_rn(__ffma2_rn(bc2(-7.5f), zc, ph), sig2), ri2);
+      nfh = __fmul2_rn(__ffma2_rn(bc2(-2.5f), zc, qh), ri2);
+    }
+    const float4 A4 = n4[k], A5 = n5[k], A6 = n6[k], A7 = n7[k];
+    const float2 B8 = n8[k];
+    const float2 bx = make_float2(A4.x, A4.y), by = make_float2(A4.z, A4.w);
+    const float2 bz = make_float2(A5.x, A5.y), mx = make_float2(A5.z, A5.w);
+    const float2 my = make_float2(A6.x, A6.y), mz = make_float2(A6.z, A6.w);
+    const float2 nbx = make_float2(A7.x, A7.y), nby = make_float2(A7.z, A7.w);
+    // velocity: alpha_j x d
+    const float2 cx = __ffma2_rn(by, dz, __fmul2_rn(B8, dy));
+    const float2 cy = __ffma2_rn(bz, dx, __fmul2_rn(nbx, dz));
+    const float2 cz = __ffma2_rn(bx, dy, __fmul2_rn(nby, dx));
+    // stretching: alpha_i x alpha_j by projection_cross, with nmu = -mu
+    const float2 nmu = __fmul2_rn(
+        __ffma2_rn(T.naz, bz, __ffma2_rn(T.nay, by, __fmul2_rn(T.nax, bx))), T.iaa);
+    const float2 vx = __fadd2_rn(__ffma2_rn(nmu, T.ax, bx), mx);
+    const float2 vy = __fadd2_rn(__ffma2_rn(nmu, T.ay, by), my);
+    const float2 vz = __fadd2_rn(__ffma2_rn(nmu, T.az, bz), mz);
+    const float2 wx = __ffma2_rn(nmu, T.nlx, __ffma2_rn(T.ay, vz, __fmul2_rn(T.naz, vy)));
+    const float2 wy = __ffma2_rn(nmu, T.nly, __ffma2_rn(T.az, vx, __fmul2_rn(T.nax, vz)));
+    const float2 wz = __ffma2_rn(nmu, T.nlz, __ffma2_rn(T.ax, vy, __fmul2_rn(T.nay, vx)));
+    const float2 t = __ffma2_rn(dz, wz, __ffma2_rn(dy, wy, __fmul2_rn(dx, wx)));
+    float2 nft = __fmul2_rn(nfh, t);
+    if (CHECK) {
+      // the target's own pair contributes nothing
+      if (2 * k == skip) qh.x = nft.x = dp.x = 0.f;
+      if (2 * k + 1 == skip) qh.y = nft.y = dp.y = 0.f;
+    }
+    a.ux = __ffma2_rn(qh, cx, a.ux);
+    a.uy = __ffma2_rn(qh, cy, a.uy);
+    a.uz = __ffma2_rn(qh, cz, a.uz);
+    a.qx = __ffma2_rn(qh, wx, a.qx);
+    a.qy = __ffma2_rn(qh, wy, a.qy);
+    a.qz = __ffma2_rn(qh, wz, a.qz);
+    a.gx = __ffma2_rn(nft, dx, a.gx);
+    a.gy = __ffma2_rn(nft, dy, a.gy);
+    a.gz = __ffma2_rn(nft, dz, a.gz);
+    if (DIFF) {
+      // delta = alpha_j - alpha_i from the hi/lo strengths
+      const float2 ex = __fadd2_rn(__fadd2_rn(bx, T.nax), __fadd2_rn(mx, T.nalx));
+      const float2 ey = __fadd2_rn(__fadd2_rn(by, T.nay), __fadd2_rn(my, T.naly));
+      const float2 ez = __fadd2_rn(__fadd2_rn(bz, T.naz), __fadd2_rn(mz, T.nalz));
+      a.ex = __ffma2_rn(dp, ex, a.ex);
+      a.ey = __ffma2_rn(dp, ey, a.ey);
+      a.ez = __ffma2_rn(dp, ez, a.ez);
+      a.ev = __ffma2_rn(dp, __fadd2_rn(T.v, make_float2(A3.z, A3.w)), a.ev);
+    }
+  }
+}
+
 __device__ __forceinline__ float box_gap2(float4 alo, float4 ahi, float4 blo, float4 bhi) {
   const float gx = fmaxf(0.f, fmaxf(alo.x - bhi.x, blo.x - ahi.x));
   const float gy = fmaxf(0.f, fmaxf(alo.y - bhi.y, blo.y - ahi.y));
@@ -992,13 +1129,20 @@ __global__ void __launch_bounds__(TB, MINB)
 // with the accurate near formulation; an item's sums go to its near slot and
 // its flag says whether it had any.  It runs before the far pass, which adds
 // the flagged slots to its own sums.
-template <int TB, int P, int R, bool DIFF, int MINB, int KERN, int NX, int NU = 2>
+// PKN: the near tiles two sources per FP32x2 instruction (tile_near_packed;
+// P = R = 1), with 1/rho^2 on uniform-radius tiles as packed mode RM gives it.
+template <int TB, int P, int R, bool DIFF, int MINB, int KERN, int NX, int NU = 2, int PKN = 0,
+          int RM = 2>
 __global__ void __launch_bounds__(TB, MINB)
     pairs_f32_near_kernel(const WorkItem *__restrict__ items, int n_items,
                           const SegDesc *__restrict__ segs, int *__restrict__ next_item) {
+  static_assert(PKN == 0 || (P == 1 && R == 1), "the packed near pass has one target per thread");
   constexpr int TG = TB / P;
   constexpr int TPB = TG * R;
+  constexpr int NQ = PKN ? TB / 2 : 1;
   __shared__ float4 sp[TB], sv[TB], spl[TB], svl[TB];
+  __shared__ float4 nq[8][NQ];  // packed near format n0..n7
+  __shared__ float2 n8[NQ];
   __shared__ int s_item;
   const int tid = threadIdx.x;
   const int g = tid % P;
@@ -1054,6 +1198,23 @@ __global__ void __launch_bounds__(TB, MINB)
       }
     }
 
+    // the target as broadcast pairs for the packed loop
+    NearT2 T2;
+    if (PKN) {
+      const float aa = fmaf(T[0].ch, T[0].ch, fmaf(T[0].bh, T[0].bh, T[0].ah * T[0].ah));
+      T2.xh = bc2(T[0].xh); T2.yh = bc2(T[0].yh); T2.zh = bc2(T[0].zh);
+      T2.xl = bc2(tpl[0].x); T2.yl = bc2(tpl[0].y); T2.zl = bc2(tpl[0].z);
+      T2.h = bc2(T[0].h);
+      T2.ax = bc2(T[0].ah); T2.ay = bc2(T[0].bh); T2.az = bc2(T[0].ch);
+      T2.nax = bc2(-T[0].ah); T2.nay = bc2(-T[0].bh); T2.naz = bc2(-T[0].ch);
+      T2.nlx = bc2(-fmaf(tvl[0].y, T[0].ch, -tvl[0].z * T[0].bh));
+      T2.nly = bc2(-fmaf(tvl[0].z, T[0].ah, -tvl[0].x * T[0].ch));
+      T2.nlz = bc2(-fmaf(tvl[0].x, T[0].bh, -tvl[0].y * T[0].ah));
+      T2.iaa = bc2(aa > 0.f ? 1.0f / aa : 0.f);
+      T2.nalx = bc2(-tvl[0].x); T2.naly = bc2(-tvl[0].y); T2.nalz = bc2(-tvl[0].z);
+      T2.v = bc2(T[0].v);
+    }
+
     bool any = false;
     const int ntiles = (w.s1 - w.s0 + TB - 1) / TB;
     for (int t = 0; t < ntiles; ++t) {
@@ -1067,7 +1228,66 @@ __global__ void __launch_bounds__(TB, MINB)
       __syncthreads();  // the previous near tile is no longer read
       stage_source(sg, ts + tid, w.s1, sp + tid, sv + tid, spl + tid, svl + tid);
       wait_staged();
+      if (PKN) {
+        // this thread's own slot, rewritten in the packed near format
+        const float4 p0 = sp[tid], p1 = sv[tid], p2 = spl[tid], p3 = svl[tid];
+        const int k = tid >> 1, hf = tid & 1;
+        float *q0 = reinterpret_cast<float *>(&nq[0][k]);
+        float *q1 = reinterpret_cast<float *>(&nq[1][k]);
+        float *q2 = reinterpret_cast<float *>(&nq[2][k]);
+        float *q3 = reinterpret_cast<float *>(&nq[3][k]);
+        float *q4 = reinterpret_cast<float *>(&nq[4][k]);
+        float *q5 = reinterpret_cast<float *>(&nq[5][k]);
+        float *q6 = reinterpret_cast<float *>(&nq[6][k]);
+        float *q7 = reinterpret_cast<float *>(&nq[7][k]);
+        float *q8 = reinterpret_cast<float *>(&n8[k]);
+        q0[hf] = -p0.x; q0[2 + hf] = -p0.y;
+        q1[hf] = -p0.z; q1[2 + hf] = p0.w;
+        q2[hf] = -p2.x; q2[2 + hf] = -p2.y;
+        q3[hf] = -p2.z; q3[2 + hf] = -p1.w;
+        q4[hf] = p1.x;  q4[2 + hf] = p1.y;
+        q5[hf] = p1.z;  q5[2 + hf] = p3.x;
+        q6[hf] = p3.y;  q6[2 + hf] = p3.z;
+        q7[hf] = -p1.x; q7[2 + hf] = -p1.y;
+        q8[hf] = -p1.z;
+      }
       __syncthreads();
+      if (PKN) {
+        const bool uni =
+            KERN == KERNEL_HIGHORDER && tlo.w == thi.w && slo.w == shi.w && tlo.w == slo.w;
+        NearAcc2 b;
+        b.ux = b.uy = b.uz = b.qx = b.qy = b.qz = b.gx = b.gy = b.gz = make_float2(0.f, 0.f);
+        b.ex = b.ey = b.ez = b.ev = make_float2(0.f, 0.f);
+        const int skip = ti[0] - ts;
+        if (diag && uni)
+          tile_near_packed<DIFF, true, true, RM, TB>(nq[0], nq[1], nq[2], nq[3], nq[4], nq[5], nq[6],
+                                                     nq[7], n8, skip, T2, slo.w, b);
+        else if (diag)
+          tile_near_packed<DIFF, true, false, RM, TB>(nq[0], nq[1], nq[2], nq[3], nq[4], nq[5], nq[6],
+                                                      nq[7], n8, skip, T2, 0.f, b);
+        else if (uni)
+          tile_near_packed<DIFF, false, true, RM, TB>(nq[0], nq[1], nq[2], nq[3], nq[4], nq[5], nq[6],
+                                                      nq[7], n8, skip, T2, slo.w, b);
+        else
+          tile_near_packed<DIFF, false, false, RM, TB>(nq[0], nq[1], nq[2], nq[3], nq[4], nq[5],
+                                                       nq[6], nq[7], n8, skip, T2, 0.f, b);
+        // undo the uniform-radius scaling; b.g holds -fh t d
+        const double As2 = uni ? A * 2.0 * (double)slo.w : A;
+        const double cd = uni ? 32.0 * cnu : cnu;
+        ou[0][0] += As2 * ((double)b.ux.x + (double)b.ux.y);
+        ou[0][1] += As2 * ((double)b.uy.x + (double)b.uy.y);
+        ou[0][2] += As2 * ((double)b.uz.x + (double)b.uz.y);
+        oa[0][0] += As2 * (((double)b.qx.x + (double)b.qx.y) - 3.0 * ((double)b.gx.x + (double)b.gx.y));
+        oa[0][1] += As2 * (((double)b.qy.x + (double)b.qy.y) - 3.0 * ((double)b.gy.x + (double)b.gy.y));
+        oa[0][2] += As2 * (((double)b.qz.x + (double)b.qz.y) - 3.0 * ((double)b.gz.x + (double)b.gz.y));
+        if (DIFF) {
+          const double v = T[0].v, ev = (double)b.ev.x + (double)b.ev.y;
+          oa[0][0] += cd * (v * ((double)b.ex.x + (double)b.ex.y) + ev * ax[0]);
+          oa[0][1] += cd * (v * ((double)b.ey.x + (double)b.ey.y) + ev * ay[0]);
+          oa[0][2] += cd * (v * ((double)b.ez.x + (double)b.ez.y) + ev * az[0]);
+        }
+        continue;
+      }
       int skip[R];
       Acc32 a[R];
 #pragma unroll
@@ -1160,6 +1380,10 @@ Kernels select_highorder(const PairConfig &c) {
   if (c.split == 1 && PAWAN_F32_MATCH(TB_, 1, 1, U_, MINB_, PK_))                         \
     return Kernels{&pairs_f32_kernel<TB_, 1, 1, U_, DIFF, MINB_, PK_, KERNEL_HIGHORDER, true>, \
                    &pairs_f32_near_kernel<TB_, 1, 1, DIFF, MINB_, KERNEL_HIGHORDER, 1>};
+#define PAWAN_F32_CASE_SPLIT2(TB_, U_, MINB_, PK_)                                       \
+  if (c.split == 2 && PAWAN_F32_MATCH(TB_, 1, 1, U_, MINB_, PK_))                         \
+    return Kernels{&pairs_f32_kernel<TB_, 1, 1, U_, DIFF, MINB_, PK_, KERNEL_HIGHORDER, true>, \
+                   &pairs_f32_near_kernel<TB_, 1, 1, DIFF, MINB_, KERNEL_HIGHORDER, 1, 2, 1, PK_>};
 #define PAWAN_F32_CASE(TB_, P_, R_, U_, MINB_) PAWAN_F32_CASE_PK(TB_, P_, R_, U_, MINB_, 0)
   PAWAN_F32_CASE_PK(128, 1, 1, 1, 4, 1)
   PAWAN_F32_CASE_PK(128, 1, 1, 2, 4, 1)
@@ -1198,6 +1422,10 @@ Kernels select_highorder(const PairConfig &c) {
   PAWAN_F32_CASE_SPLIT(256, 4, 2, 2)
   PAWAN_F32_CASE_SPLIT(128, 4, 4, 1)
   PAWAN_F32_CASE_SPLIT(128, 4, 4, 2)
+  PAWAN_F32_CASE_SPLIT2(256, 4, 2, 1)
+  PAWAN_F32_CASE_SPLIT2(256, 4, 2, 2)
+  PAWAN_F32_CASE_SPLIT2(128, 4, 4, 1)
+  PAWAN_F32_CASE_SPLIT2(128, 4, 4, 2)
   return Kernels{};
 }
 
@@ -1215,6 +1443,7 @@ Kernels select_gaussian(const PairConfig &c) {
 #undef PAWAN_F32_CASE_PK
 #undef PAWAN_F32_CASE_K
 #undef PAWAN_F32_CASE_SPLIT
+#undef PAWAN_F32_CASE_SPLIT2
 #undef PAWAN_F32_MATCH
 
 Kernels select(const PairConfig &c, bool diffusion, int kernel) {

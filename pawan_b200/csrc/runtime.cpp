@@ -60,14 +60,16 @@ std::vector<TileChoice> tile_candidates(int precision, int kernel) {
         t.pc = PairConfig{tb, sh[0], sh[2], sh[1], sh[3], sh[4]};
         if (pairs_f32_supported(t.pc, kernel)) v.push_back(t);
       }
-    // the packed unroll-4 shapes again with a separate near pass (ahead where
-    // near tile pairs are many: ragged batches of small rings, scrambled states)
-    for (int tb : {128, 256})
-      for (int pk : {1, 2}) {
-        TileChoice t;
-        t.pc = PairConfig{tb, 1, 4, 1, 0, pk, 1};
-        if (pairs_f32_supported(t.pc, kernel)) v.push_back(t);
-      }
+    // the packed unroll-4 shapes again with a separate near pass, scalar (1) or
+    // packed (2) (ahead where near tile pairs are many: ragged batches of small
+    // rings, scrambled states)
+    for (int split : {1, 2})
+      for (int tb : {128, 256})
+        for (int pk : {1, 2}) {
+          TileChoice t;
+          t.pc = PairConfig{tb, 1, 4, 1, 0, pk, split};
+          if (pairs_f32_supported(t.pc, kernel)) v.push_back(t);
+        }
   } else {
     for (int tb : {128, 256}) {
       TileChoice t;

@@ -99,11 +99,17 @@ def test_coincident_particles_give_nan_where_the_reference_does(ctx, prec):
     assert sorted(np.flatnonzero(bad)) == [7, 40, 100, 250]
     s = System(ctx, [n], 1e-3, prec)
     s.set_particles(pos, vor, rad, vol)
-    s.solve()
-    u, da = s.union_rates()
-    assert np.array_equal(np.isnan(u).all(axis=1) & np.isnan(da).all(axis=1), bad)
-    assert np.isfinite(u[~bad]).all() and np.isfinite(da[~bad]).all()
-    check(prec, u[~bad], da[~bad], u_ref[~bad], da_ref[~bad])
+    # FP32: the default tiling, then the scalar and the packed near pass
+    configs = [None] + ([dict(threads=128, unroll=4, packed=2, split_near=sp) for sp in (1, 2)]
+                        if prec == "f32" else [])
+    for cfg in configs:
+        if cfg:
+            s.set_config(**cfg)
+        s.solve()
+        u, da = s.union_rates()
+        assert np.array_equal(np.isnan(u).all(axis=1) & np.isnan(da).all(axis=1), bad), cfg
+        assert np.isfinite(u[~bad]).all() and np.isfinite(da[~bad]).all(), cfg
+        check(prec, u[~bad], da[~bad], u_ref[~bad], da_ref[~bad])
 
 
 def test_many_wakes_union(ctx):
@@ -265,11 +271,11 @@ TUNE_CANDIDATES = [(tb,) + sh + (0,) for tb in (128, 256) for sh in (
     (1, 1, 4, 5, 0), (1, 1, 1, 0, 1), (1, 1, 2, 0, 1), (1, 1, 4, 0, 1), (1, 1, 2, 5, 1),
     (1, 1, 2, 0, 2), (1, 1, 4, 0, 2))
     if not (tb == 256 and sh in ((1, 1, 4, 5, 0), (1, 1, 1, 0, 1), (1, 1, 2, 5, 1)))]
-# ... and with a separate near pass (the last field)
-TUNE_CANDIDATES += [(tb, 1, 1, 4, 0, pk, 1) for tb in (128, 256) for pk in (1, 2)]
+# ... and with a separate near pass (the last field: 1 scalar, 2 packed)
+TUNE_CANDIDATES += [(tb, 1, 1, 4, 0, pk, sp) for sp in (1, 2) for tb in (128, 256) for pk in (1, 2)]
 # the tiling the default bench run's autotuner picks on the ring pair, and the
 # library's default tiling
-TIMED_TILING = (256, 1, 1, 4, 0, 1, 0)
+TIMED_TILING = (256, 1, 1, 4, 0, 2, 0)
 DEFAULT_TILING = (128, 1, 1, 4, 0, 2, 0)
 FULL_SAMPLES = 4096
 
@@ -318,7 +324,7 @@ def test_full_size_every_candidate_tiling(full, name, tiling):
 @pytest.mark.parametrize("tiling", [TIMED_TILING, DEFAULT_TILING], ids=["timed", "default"])
 @pytest.mark.parametrize("name", ["ring_pair", "helical_wake"])
 def test_full_size_timed_tiling_every_chunking(full, name, tiling, ips):
-    """The bench's autotuned tiling (256 threads, packed mode 1) and the
+    """The bench's autotuned tiling (256 threads, packed mode 2) and the
     library default (128 threads, mode 2) at every chunking the autotuner
     times, at full size against the FP64 restatement."""
     _check_full(full, name, tiling, ips)
@@ -372,6 +378,9 @@ def test_tile_classes_at_their_boundaries(ctx, gap, mixed):
                     blocks_per_sm=minb, packed=mode) for tb, unroll, minb, mode in F32_PACKED[:4]]
     configs += [dict(threads=tb, threads_per_target=p, unroll=unroll, items_per_slot=16,
                      targets_per_thread=r, blocks_per_sm=minb) for tb, p, r, unroll, minb in F32_TILINGS[:6]]
+    # the separate near pass, scalar and packed
+    configs += [dict(threads=128, unroll=4, items_per_slot=16, packed=mode, split_near=sp)
+                for sp in (1, 2) for mode in (1, 2)]
     for cfg in configs:
         sysm.set_config(**cfg)
         sysm.set_states(st1)
@@ -387,9 +396,9 @@ def test_tile_classes_at_their_boundaries(ctx, gap, mixed):
 
 
 @pytest.mark.parametrize("tiling", [TIMED_TILING, DEFAULT_TILING, (128, 2, 1, 4, 0, 0, 0), (128, 1, 2, 2, 0, 0, 0),
-                                    (256, 1, 1, 4, 0, 1, 1)],
+                                    (256, 1, 1, 4, 0, 1, 1), (256, 1, 1, 4, 0, 2, 2), (128, 1, 1, 4, 0, 1, 2)],
                          ids=["timed", "default", "two-threads-per-target", "two-targets-per-thread",
-                              "near-pass"])
+                              "near-pass", "packed-near-pass", "packed-near-pass-128"])
 def test_chunk_sums_inside_the_launch(ctx, tiling):
     """The pair kernels sum a target tile's chunk partials inside the launch
     (the block completing the tile, in chunk order).  With the tiling fixed,
