@@ -549,10 +549,12 @@ def run_serving_leg(ctx, rate: float, duration: float, n_lo: int, n_hi: int, ste
         time.sleep(0.01)
     elapsed = time.perf_counter() - t0
     st = srv.stats()
+    engine_tiling = srv.tiling()
     srv.close()
     lat.sort()
     pct = (lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None)
-    accuracy = serving_accuracy(ctx, finished, accuracy_sample) if accuracy_sample and finished else None
+    accuracy = (serving_accuracy(ctx, finished, accuracy_sample, engine_tiling)
+                if accuracy_sample and finished else None)
     return {"accuracy": accuracy, "policy": policy, "rate_per_s": rate, "arrival_window_s": duration, "arrivals": len(reqs),
             "N_range": [n_lo, n_hi], "steps_range": [steps_lo, steps_hi],
             "budget_bytes": budget, "max_step_interactions": cap, "max_active": max_active,
@@ -567,10 +569,11 @@ def run_serving_leg(ctx, rate: float, duration: float, n_lo: int, n_hi: int, ste
             "elapsed_s": elapsed, "arrival_replay_s": t_arrivals}
 
 
-def serving_accuracy(ctx, finished, k: int) -> dict:
+def serving_accuracy(ctx, finished, k: int, tiling: dict) -> dict:
     """Served results of k completed requests against the same request run
-    alone (FP32, its own system and plan) and on the FP64 path, plus one
-    right-hand side of each at its initial state in FP32 against FP64."""
+    alone (FP32, its own system and plan, with the engine's tiling) and on the
+    FP64 path, plus one right-hand side of each at its initial state in FP32
+    against FP64."""
     from pawan_b200 import System
     from pawan_b200 import geometry as g
     pick = [finished[i] for i in np.linspace(0, len(finished) - 1, min(k, len(finished))).astype(int)]
@@ -584,6 +587,8 @@ def serving_accuracy(ctx, finished, k: int) -> dict:
         for prec in ("f32", "f64"):
             x = System(ctx, counts, r.scenario.nu, prec)
             x.set_particles(pos, vor, rad, vol)
+            if prec == "f32":
+                x.set_config(**tiling)
             if not runs:
                 initials.append(x.get_states())
             x.solve()
@@ -598,7 +603,8 @@ def serving_accuracy(ctx, finished, k: int) -> dict:
     return {"requests": len(pick), "N": sizes,
             "served_vs_alone_fp32": dict(_increment_errors(served, solo32, initials),
                                          metric="state increment of the served result against the same "
-                                                "request run alone (FP32, its own plan)"),
+                                                "request run alone (FP32, its own plan, the engine's "
+                                                "tiling)"),
             "rhs_fp32_vs_fp64_gpu": dict(_rhs_errors(rhs32, rhs64),
                                          metric="one right-hand side at the request's initial state"),
             "trajectory_vs_fp64_gpu": dict(_increment_errors(served, solo64, initials), note=TRAJECTORY_NOTE),

@@ -325,6 +325,11 @@ int pawan_server_fetch(pawan_server *srv, long long id, double *state, size_t si
                        double *t_submit, double *t_admit, double *t_done);
 int pawan_server_cancel(pawan_server *srv, long long id);
 int pawan_server_stats(pawan_server *srv, pawan_serve_stats *out);
+/* The tiling the engine's pair launches use (FP32: 128 threads, packed far
+ * path mode 1, the packed near pass; sources in fixed 8,192-source chunks, so
+ * items_per_slot is not used), for running a request alone with the same
+ * arithmetic. */
+int pawan_server_get_tiling(pawan_server *srv, pawan_tiling *out);
 /* Host-side fault injection, for testing how callers and the engine recover
  * (no GPU fault is made).  PAWAN_FAULT_ALLOC: the next `count` admissions
  * fail as an out-of-memory from the device allocator would (the request is

@@ -155,6 +155,7 @@ _SIGS = {
     "pawan_server_fetch": (ctypes.c_int, [_vp, ctypes.c_longlong, _dp, ctypes.c_size_t, _dp, _dp, _dp]),
     "pawan_server_cancel": (ctypes.c_int, [_vp, ctypes.c_longlong]),
     "pawan_server_stats": (ctypes.c_int, [_vp, ctypes.POINTER(ServeStats)]),
+    "pawan_server_get_tiling": (ctypes.c_int, [_vp, ctypes.POINTER(Tiling)]),
     "pawan_interact_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.c_size_t, ctypes.c_double, ctypes.c_void_p,
                                               ctypes.c_void_p, ctypes.c_void_p]),
@@ -617,6 +618,15 @@ class Server:
         if st != OK:
             raise PawanError(st, "stats")
         return {f: getattr(s, f) for f, _ in ServeStats._fields_}
+
+    def tiling(self) -> dict:
+        """The tiling of the engine's pair launches (System.set_config
+        keywords), to run a request alone with the same arithmetic."""
+        t = Tiling()
+        st = self._lib.pawan_server_get_tiling(self._h, ctypes.byref(t))
+        if st != OK:
+            raise PawanError(st, "tiling")
+        return {f: getattr(t, f) for f, _ in Tiling._fields_}
 
 
 NOALLOC_MAX_PARTICLES = 16384

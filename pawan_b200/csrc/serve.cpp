@@ -89,12 +89,26 @@ struct Request {
 // Device bytes a request holds while active: the system's buffers plus its
 // rates and partial slots in a batched plan (fixed chunk size; slots cover
 // whole target tiles of at most 512 particles).
-double request_bytes(size_t n, int tb) {
+double request_bytes(size_t n, const TileChoice &tile) {
+  const int tb = tile.pc.tb;
   const double per = 5 * 48.0 + 16.0 + 4.0 + 64.0 + 64.0 + 1.0 + 48.0;
   const size_t chunk = ((kServeChunkSources + tb - 1) / tb) * (size_t)tb;
   const size_t nch = (n + chunk - 1) / chunk;
   const double slots = nch > 1 ? 48.0 * (double)(n + 512) * (double)nch : 0.0;
-  return (double)n * per + slots + 4096.0;
+  // a separate near pass keeps its sums in slots of its own (every chunk, one
+  // chunk included) with a flag byte each
+  const double near = tile.pc.split > 0 ? 49.0 * (double)(n + 512) * (double)nch : 0.0;
+  return (double)n * per + slots + near + 4096.0;
+}
+
+// The engine's tiling: for FP32 the packed far path with the packed near pass
+// (requests are rings of a few thousand to a few hundred thousand particles,
+// where the near tile pairs are a tenth of the work for the small ones); the
+// library default otherwise.
+TileChoice serve_tile(int precision) {
+  TileChoice t = default_tile(precision);
+  if (precision == PAWAN_PREC_F32) t.pc = PairConfig{128, 1, 4, 1, 0, 1, 2};
+  return t;
 }
 
 }  // namespace
@@ -406,6 +420,20 @@ void worker_main(pawan_server *srv) {
 
 extern "C" {
 
+int pawan_server_get_tiling(pawan_server *srv, pawan_tiling *out) {
+  if (!srv || !out) return PAWAN_ERR_INVALID;
+  const TileChoice &t = srv->tile;
+  out->threads = t.pc.tb;
+  out->threads_per_target = t.pc.p;
+  out->targets_per_thread = t.pc.r;
+  out->unroll = t.pc.unroll;
+  out->blocks_per_sm = t.pc.minb;
+  out->packed = t.pc.packed;
+  out->split_near = t.pc.split;
+  out->items_per_slot = t.items_per_slot;
+  return PAWAN_OK;
+}
+
 int pawan_server_create(pawan_ctx *ctx, const pawan_serve_config *cfg, pawan_server **out) {
   if (!ctx || !cfg || !out) return PAWAN_ERR_INVALID;
   if (!(cfg->budget_bytes > 0) || cfg->precision < PAWAN_PREC_F32 ||
@@ -414,7 +442,7 @@ int pawan_server_create(pawan_ctx *ctx, const pawan_serve_config *cfg, pawan_ser
     return fail(ctx, PAWAN_ERR_INVALID, "bad serving configuration");
   std::unique_ptr<pawan_server> srv(new pawan_server());
   srv->cfg = *cfg;
-  srv->tile = default_tile(cfg->precision);
+  srv->tile = serve_tile(cfg->precision);
   int st = pawan_ctx_create(ctx->device, &srv->ctx);
   if (st != PAWAN_OK) return fail(ctx, st, "cannot create the serving context");
   // freed request memory stays in the device's pool for the next admission
@@ -478,7 +506,7 @@ int pawan_server_submit(pawan_server *srv, size_t n_wakes, const size_t *num_par
   r->nu = nu;
   r->dt = dt;
   r->nsteps = nsteps;
-  r->bytes = request_bytes(n, srv->tile.pc.tb);
+  r->bytes = request_bytes(n, srv->tile);
   std::lock_guard<std::mutex> lk(srv->mu);
   r->id = srv->next_id++;
   r->t_submit = now_since(srv->t0);

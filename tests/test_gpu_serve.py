@@ -43,13 +43,17 @@ def test_alone_and_in_the_mix_are_identical(ctx):
         assert srv.wait(rid, 120)
     mixed = [srv.fetch(rid) for rid in ids]
     stats = srv.stats()
+    tiling = srv.tiling()
     srv.close()
     assert stats["completed"] == len(scs) and stats["rejected"] == 0
     for sc, (out, ts, ta, td) in zip(scs, mixed):
         assert out is not None and ts <= ta <= td
         alone = run_alone(ctx, sc)
         assert np.array_equal(out, alone)
+        # a system of its own with the engine's tiling: the same FP32 tile sums,
+        # grouped differently in FP64
         solo = System.from_scenario(ctx, sc, "f32")
+        solo.set_config(**tiling)
         solo.rk4(sc.dt, sc.steps)
         st0 = sc.state()
         assert rms_rel(out - st0, solo.get_states() - st0) < 1e-12
