@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--strong", action="store_true",
                     help="one system sharded over the ranks (all-gather per RK4 stage) instead of "
                          "one replica per rank")
+    ap.add_argument("--batch-rhs", action="store_true",
+                    help="profiling aid: right-hand sides of the 512-solve ragged batch only (the "
+                         "autotuned tiling, or --tile), timed with CUDA events; one JSON line")
     ap.add_argument("--tile", default=None,
                     help="fixed FP32 tiling instead of the autotuned one: threads,threads_per_target,"
                          "targets_per_thread,unroll,blocks_per_sm,packed[,items_per_slot[,split_near]]")
@@ -975,10 +978,55 @@ def run_configs(args):
     ctx.close()
 
 
+def run_batch_rhs(args):
+    """Right-hand sides of the 512-solve ragged batch (one launch sequence per
+    RHS over every solve), the profiling counterpart of the batched leg:
+    `--warmup` untimed, then `--steps` timed with CUDA events on the library's
+    stream."""
+    import pawan_b200
+    from pawan_b200 import Batch, System
+    from pawan_b200 import geometry as g
+    ctx = pawan_b200.Context(0)
+    scs = g.ragged_batch()
+    systems = [System.from_scenario(ctx, sc, "f32") for sc in scs]
+    b = Batch(ctx, systems)
+    if args.tile:
+        v = [int(x) for x in args.tile.split(",")]
+        tb, p, r, unroll, minb, packed = v[:6]
+        ips = v[6] if len(v) > 6 else 32
+        split = v[7] if len(v) > 7 else 0
+        b.set_config(tb, p, unroll, ips, targets_per_thread=r, blocks_per_sm=minb, packed=packed,
+                     split_near=split)
+        tiling = args.tile
+    else:
+        b.autotune()
+        tiling = "autotuned"
+    for _ in range(max(1, args.warmup)):
+        b.solve()
+    ctx.synchronize()
+    ctx.profile(True)
+    for _ in range(args.steps):
+        b.solve()
+    ctx.synchronize()
+    r = ctx.profile_read()
+    ctx.profile(False)
+    ms = r["pair_ms"] / max(1, r["pair_launches"])
+    print(json.dumps({"workload": "ragged batch, 512 solves, one right-hand side", "tiling": tiling,
+                      "solves": len(scs), "interactions_per_rhs": sum(float(sc.n) ** 2 for sc in scs),
+                      "ms_per_rhs": ms, "G_interactions_per_s": r["pair_interactions"] / r["pair_ms"] / 1e6}))
+    b.close()
+    for x in systems:
+        x.close()
+    ctx.close()
+
+
 def main():
     args = parse()
     if args.configs:
         run_configs(args)
+        return
+    if args.batch_rhs:
+        run_batch_rhs(args)
         return
     rk = Ranks(args.gpus)
     try:
