@@ -223,6 +223,14 @@ __device__ __forceinline__ void kernel_scalars_series(float sig2, float r2, floa
 // come from their power series in y = -x2/2,
 //   gq = K sum_m y^m / (m! (2m+3)),   gf = -K sum_m y^m / (m! (2m+5)),
 // nine terms (relative truncation error < 1e-8 at x2 = 1).
+// Far field of the Gaussian kernel (gauss_far): where every pair of a tile pair
+// has x = rho/sigma >= 7 (checked on the tiles' boxes), e = exp(-x2/2) <=
+// 2.3e-11 and erf(x/sqrt 2) = 1 - 2.6e-12, so gq = 1/x^3 to 1.3e-10 relative
+// (K e x against 1), gf = -3/x^5 to 2.1e-9 (K e x^3/3 against 1) and dp is 0
+// at FP32 resolution:
+//   qh = rho^-3,   fh = -rho^-5 = -qh / rho^2,   dp = 0,
+// the singular field, one MUFU rsqrt and three multiplies per pair in place of
+// an exp and an erf (the far loops' series branches with KERN = Gaussian).
 __device__ __forceinline__ void gauss_scalars(float sig2, float r2, float ri, float &qh, float &fh,
                                               float &dp) {
   const float K = 0.797884561f;
@@ -291,9 +299,15 @@ __device__ __forceinline__ void tile_far(const float4 *__restrict__ sa,
       const float r2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
       float qh, fh, dp;
       if (NZ && SER) {
-        // Z-free far field by the series (kernel_scalars_series)
+        // Z-free far field by the series (kernel_scalars_series), or the
+        // Gaussian kernel's far field (gauss_far)
         float nfh;
-        if (UNI) {
+        if (KERN == KERNEL_GAUSSIAN) {
+          const float ri = rsqrtf(r2);
+          const float ri2 = ri * ri;
+          qh = ri * ri2;
+          nfh = qh * ri2;
+        } else if (UNI) {
           const float ri = rsqrtf(r2);
           const float ri2 = ri * ri;
           qh = ri * ri2 * fmaf(-hu, ri2, 1.0f) * ri2;
@@ -423,7 +437,10 @@ __device__ __forceinline__ void tile_far_packed(const float4 *__restrict__ f0,
       // 1), 5 FP32x2 operations with one radius (6 when RM = 2)
       const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
       const float2 ri2 = inv_r2<RM>(r2, ri);
-      if (UNI) {
+      if (KERN == KERNEL_GAUSSIAN) {
+        // the Gaussian kernel's far field (gauss_far): qh = rho^-3
+        qh = __fmul2_rn(ri, ri2);
+      } else if (UNI) {
         qh = __fmul2_rn(__fmul2_rn(__fmul2_rn(ri, ri2), __ffma2_rn(nh2, ri2, one2)), ri2);
       } else {
         const float2 e = __fmul2_rn(__fadd2_rn(T.h, hj), ri2);
@@ -898,9 +915,12 @@ __global__ void __launch_bounds__(TB, MINB)
       const bool near = diag || !far_tiles(gap2, slo, shi, sg.near2);
       // every pair at rho >= 6 sigma: the Z-free far field (w of a box = the
       // range of h = s^2/2, so thi.w + shi.w is the largest sigma^2)
-      const bool nz = KERN == KERNEL_HIGHORDER && !near && gap2 >= 36.f * (thi.w + shi.w);
+      // Gaussian kernel, every pair at rho >= 7 sigma: its far field (gauss_far),
+      // taken by the series branches of the far loops
+      const bool gfar = KERN == KERNEL_GAUSSIAN && !near && gap2 >= 49.f * (thi.w + shi.w);
+      const bool nz = (KERN == KERNEL_HIGHORDER && !near && gap2 >= 36.f * (thi.w + shi.w)) || gfar;
       // every pair at rho >= 16 sigma: the Z-free field by its series
-      const bool ser = nz && gap2 >= 256.f * (thi.w + shi.w);
+      const bool ser = (nz && gap2 >= 256.f * (thi.w + shi.w)) || gfar;
       // one smoothing radius over both tiles
       const bool uni = KERN == KERNEL_HIGHORDER && tlo.w == thi.w && slo.w == shi.w && tlo.w == slo.w;
       const float cx = 0.5f * (slo.x + shi.x), cy = 0.5f * (slo.y + shi.y),

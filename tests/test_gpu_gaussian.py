@@ -86,3 +86,48 @@ def test_gaussian_rk4_matches_oracle_and_switching_back(ctx):
     s.set_states(st0)
     s.solve()
     check("f32", *s.union_rates(), *oracle.pairs(pos, vor, rad, vol, sc.nu))
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+@pytest.mark.parametrize("gap", [6.0, 7.5, 10.0])
+def test_gaussian_far_class_at_its_boundary(ctx, gap, mixed):
+    """Two compact clusters of 256 particles whose boxes are `gap` smoothing
+    radii apart: below 7 sigma the Gaussian far tiles evaluate exp and erf,
+    from 7 sigma on (8.4 s with radii in [0.8 s, 1.2 s]) the singular field
+    they equal there to FP32 resolution.  The cross-cluster part at cluster A
+    on its own (by linearity: B's strengths doubled, minus the first solve)
+    against the same difference in the FP64 oracle, on every compiled
+    Gaussian tiling; B's strengths share a direction so that the part is well
+    conditioned."""
+    rng = np.random.default_rng(int(gap * 10) + 1)
+    s = 0.05
+    n = 256
+    a = rng.uniform(-0.5 * s, 0.5 * s, (n, 3))
+    b = rng.uniform(-0.5 * s, 0.5 * s, (n, 3))
+    b[:, 0] += (gap + 1.0) * s  # box gap = gap * s
+    pos = np.concatenate([a, b])
+    vor = rng.normal(size=(2 * n, 3)) * 1e-3
+    vor[n:] += np.array([1e-3, 2e-3, -1.5e-3])
+    vor2 = vor.copy()
+    vor2[n:] *= 2.0
+    rad = s * rng.uniform(0.8, 1.2, 2 * n) if mixed else np.full(2 * n, s)
+    vol = np.full(2 * n, 1e-5)
+    nu = 1e-3
+    u1, da1 = oracle.pairs(pos, vor, rad, vol, nu, kernel="gaussian")
+    u2, da2 = oracle.pairs(pos, vor2, rad, vol, nu, kernel="gaussian")
+    du_ref, dda_ref = (u2 - u1)[:n], (da2 - da1)[:n]
+    st1, st2 = union_to_state([2 * n], pos, vor), union_to_state([2 * n], pos, vor2)
+    sysm = gauss_system(ctx, [2 * n], pos, vor, rad, vol, nu, "f32")
+    for tb, p, r, unroll, minb, packed in [(128, 1, 1, 4, 0, 2), (128, 1, 1, 2, 0, 0), (128, 2, 1, 4, 0, 0),
+                                          (256, 1, 1, 4, 0, 2)]:
+        sysm.set_config(tb, p, unroll, 16, targets_per_thread=r, blocks_per_sm=minb, packed=packed)
+        sysm.set_states(st1)
+        sysm.solve()
+        ug1, dag1 = sysm.union_rates()
+        check("f32", ug1, dag1, u1, da1)
+        sysm.set_states(st2)
+        sysm.solve()
+        ug2, dag2 = sysm.union_rates()
+        du, dda = (ug2 - ug1)[:n], (dag2 - dag1)[:n]
+        assert rms_rel(du, du_ref) < 1e-5 and rms_rel(dda, dda_ref) < 1e-5, \
+            (tb, p, packed, rms_rel(du, du_ref), rms_rel(dda, dda_ref))
