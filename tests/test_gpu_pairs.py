@@ -71,6 +71,15 @@ def test_ragged_sizes_against_restatement(ctx, n):
         s.set_particles(pos, vor, rad, vol)
         s.solve()
         check(prec, *s.union_rates(), u_ref, da_ref)
+    # FP32 through both near passes (random radii: the general scalars; ragged
+    # last tiles: sources past the end staged as far, zero-strength particles)
+    s = System(ctx, [n], 1e-3, "f32")
+    s.set_particles(pos, vor, rad, vol)
+    for tb in (128, 256):
+        for split in (1, 2):
+            s.set_config(threads=tb, unroll=4, packed=1, split_near=split)
+            s.solve()
+            check("f32", *s.union_rates(), u_ref, da_ref)
 
 
 @pytest.mark.parametrize("prec", PRECS)
@@ -153,6 +162,12 @@ def test_every_packed_f32_tiling(ctx, tb, unroll, minb, mode):
             s.set_config(tb, 1, unroll, ips, blocks_per_sm=minb, packed=mode)
             s.solve()
             check("f32", *s.union_rates(), u_ref, da_ref)
+        if unroll == 4 and minb == 0:
+            # the same with the near tile pairs in a pass of their own, scalar and packed
+            for split in (1, 2):
+                s.set_config(tb, 1, unroll, 16, packed=mode, split_near=split)
+                s.solve()
+                check("f32", *s.union_rates(), u_ref, da_ref)
 
 
 @pytest.mark.parametrize("tb,p,r,unroll,minb", F32_TILINGS)
