@@ -104,8 +104,10 @@ template <int KERN>
 __global__ void __launch_bounds__(kInfThreads)
     influence_columns_kernel(int n, int ncols, const double4 *__restrict__ pos,
                              const double *__restrict__ cols, double *__restrict__ field) {
+  // sources' positions, and each column's strengths one double4 per source
+  // (x, y, z, unused) so that a source's three components are one load
   __shared__ double4 sp[kInfThreads];
-  __shared__ double sa[kColGroup][3 * kInfThreads];
+  __shared__ double4 sa[kColGroup][kInfThreads];
   const int tid = threadIdx.x;
   const int i = blockIdx.x * kInfThreads + tid;
   const int c0 = blockIdx.y * kColGroup;
@@ -122,7 +124,8 @@ __global__ void __launch_bounds__(kInfThreads)
     if (tid < cnt) sp[tid] = pos[ts + tid];
     for (int c = 0; c < nc; ++c) {
       const double *src = cols + ((size_t)(c0 + c) * n + ts) * 3;
-      for (int e = tid; e < 3 * cnt; e += kInfThreads) sa[c][e] = src[e];
+      double *dst = reinterpret_cast<double *>(sa[c]);
+      for (int e = tid; e < 3 * cnt; e += kInfThreads) dst[4 * (e / 3) + e % 3] = src[e];
     }
     __syncthreads();
     for (int jj = 0; jj < cnt; ++jj) {
@@ -130,9 +133,10 @@ __global__ void __launch_bounds__(kInfThreads)
 #pragma unroll
       for (int c = 0; c < kColGroup; ++c) {
         if (c < nc) {
-          k[c][0] = __fma_rn(z, sa[c][3 * jj], k[c][0]);
-          k[c][1] = __fma_rn(z, sa[c][3 * jj + 1], k[c][1]);
-          k[c][2] = __fma_rn(z, sa[c][3 * jj + 2], k[c][2]);
+          const double4 a = sa[c][jj];
+          k[c][0] = __fma_rn(z, a.x, k[c][0]);
+          k[c][1] = __fma_rn(z, a.y, k[c][1]);
+          k[c][2] = __fma_rn(z, a.z, k[c][2]);
         }
       }
     }
