@@ -131,3 +131,21 @@ def test_gaussian_far_class_at_its_boundary(ctx, gap, mixed):
         du, dda = (ug2 - ug1)[:n], (dag2 - dag1)[:n]
         assert rms_rel(du, du_ref) < 1e-5 and rms_rel(dda, dda_ref) < 1e-5, \
             (tb, p, packed, rms_rel(du, du_ref), rms_rel(dda, dda_ref))
+
+
+@pytest.mark.parametrize("tiling", [(256, 1, 1, 4, 0, 2), (128, 1, 1, 2, 0, 0)])
+def test_gaussian_full_size_sampled_targets(ctx, tiling):
+    """The ring pair at full size (N = 131,072) with the Gaussian kernel, where
+    nearly every tile pair takes the far class: 4,096 sampled targets against
+    the FP64 restatement summed over all N sources, packed and scalar far
+    loops."""
+    sc = g.ring_pair(steps=1)
+    pos, vor, rad, vol = sc.union()
+    t = np.sort(np.random.default_rng(1).choice(sc.n, 4096, replace=False))
+    u_ref, da_ref = oracle.pairs(pos, vor, rad, vol, sc.nu, targets=t, kernel="gaussian")
+    s = gauss_system(ctx, sc.counts, pos, vor, rad, vol, sc.nu, "f32")
+    tb, p, r, unroll, minb, packed = tiling
+    s.set_config(tb, p, unroll, 64, targets_per_thread=r, blocks_per_sm=minb, packed=packed)
+    s.solve()
+    u, da = s.union_rates()
+    check("f32", u[t], da[t], u_ref, da_ref)
