@@ -1,7 +1,9 @@
 // All-pairs interaction in FP64 with the kernel algebra of the FP32 kernel
-// (pair_f32.cu): two rsqrt per pair, no pow, no division; the stretching and
-// diffusion vectors per pair as the reference forms them (alpha_i x alpha_j,
-// v_i alpha_j - v_j alpha_i).  This is the
+// (pair_f32.cu): two rsqrt per pair, no pow, no division.  Sums that factor
+// out of the pair loop are taken after it: the q-term of the stretching as
+// alpha_i x (sum q alpha_j), the F-term's triple product d.(alpha_i x alpha_j)
+// as alpha_i.(alpha_j x d) from the velocity's cross product, and the
+// diffusion as v_i sum(Dp alpha_j) - alpha_i sum(Dp v_j).  This is the
 // "tuned FP64" variant, reported beside the FP32 kernel and the plain FP64
 // comparator (pair_plain.cu).  Same work items, partial layout and gather form.
 //
@@ -72,8 +74,11 @@ __global__ void __launch_bounds__(TB)
       vi = sg.vor64[i];
     }
     const double hi = 0.5 * pi.w * pi.w;
+    // u = sum qh (alpha_j x d); Q = sum qh alpha_j (the q-term of the
+    // stretching is alpha_i x Q); G = sum fh [alpha_i.(alpha_j x d)] d;
+    // E = sum Dp alpha_j, V = sum Dp v_j (the diffusion is v_i E - V alpha_i)
     double ux = 0, uy = 0, uz = 0, qx = 0, qy = 0, qz = 0, gx = 0, gy = 0, gz = 0;
-    double ex = 0, ey = 0, ez = 0;
+    double ex = 0, ey = 0, ez = 0, ev = 0;
 
     const int ntiles = (w.s1 - w.s0 + TB - 1) / TB;
     double4 rp, rv;
@@ -111,13 +116,12 @@ __global__ void __launch_bounds__(TB)
           qh = fma(-7.5, zc, ph) * sig2 * ri2;
           fh = fma(2.5, zc, -qh) * ri2;
         }
+        // alpha_j x d, for the velocity and (dotted with alpha_i) for the
+        // triple product d.(alpha_i x alpha_j) = alpha_i.(alpha_j x d)
         const double cx = fma(s.y, dz, -s.z * dy);
         const double cy = fma(s.z, dx, -s.x * dz);
         const double cz = fma(s.x, dy, -s.y * dx);
-        const double wx = fma(vi.y, s.z, -vi.z * s.y);
-        const double wy = fma(vi.z, s.x, -vi.x * s.z);
-        const double wz = fma(vi.x, s.y, -vi.y * s.x);
-        const double tt = fma(dz, wz, fma(dy, wy, dx * wx));
+        const double tt = fma(vi.z, cz, fma(vi.y, cy, vi.x * cx));
         double ft = fh * tt;
         const bool self = (jj == skip);
         qh = self ? 0.0 : qh;
@@ -126,30 +130,36 @@ __global__ void __launch_bounds__(TB)
         ux = fma(qh, cx, ux);
         uy = fma(qh, cy, uy);
         uz = fma(qh, cz, uz);
-        qx = fma(qh, wx, qx);
-        qy = fma(qh, wy, qy);
-        qz = fma(qh, wz, qz);
+        qx = fma(qh, s.x, qx);
+        qy = fma(qh, s.y, qy);
+        qz = fma(qh, s.z, qz);
         gx = fma(ft, dx, gx);
         gy = fma(ft, dy, gy);
         gz = fma(ft, dz, gz);
         if (DIFF) {
-          ex = fma(dp, fma(vi.w, s.x, -s.w * vi.x), ex);
-          ey = fma(dp, fma(vi.w, s.y, -s.w * vi.y), ey);
-          ez = fma(dp, fma(vi.w, s.z, -s.w * vi.z), ez);
+          ex = fma(dp, s.x, ex);
+          ey = fma(dp, s.y, ey);
+          ez = fma(dp, s.z, ez);
+          ev = fma(dp, s.w, ev);
         }
       }
     }
 
     if (valid) {
       const double A = kInv4Pi;
-      double dax = A * qx + 3.0 * A * gx;
-      double day = A * qy + 3.0 * A * gy;
-      double daz = A * qz + 3.0 * A * gz;
+      // alpha_i x Q
+      const double wx = fma(vi.y, qz, -vi.z * qy);
+      const double wy = fma(vi.z, qx, -vi.x * qz);
+      const double wz = fma(vi.x, qy, -vi.y * qx);
+      double dax = A * wx + 3.0 * A * gx;
+      double day = A * wy + 3.0 * A * gy;
+      double daz = A * wz + 3.0 * A * gz;
       if (DIFF) {
+        // v_i E - V alpha_i
         const double c = 15.0 * sg.nu * A;
-        dax += c * ex;
-        day += c * ey;
-        daz += c * ez;
+        dax += c * fma(vi.w, ex, -ev * vi.x);
+        day += c * fma(vi.w, ey, -ev * vi.y);
+        daz += c * fma(vi.w, ez, -ev * vi.z);
       }
       const ItemOut o = item_out(sg, w.t0, w.chunk, TB);
       double *out = o.base + (i - w.t0);
