@@ -1,9 +1,11 @@
 // All-pairs interaction in FP64 with the kernel algebra of the FP32 kernel
-// (pair_f32.cu): two rsqrt per pair, no pow, no division.  Sums that factor
-// out of the pair loop are taken after it: the q-term of the stretching as
-// alpha_i x (sum q alpha_j), the F-term's triple product d.(alpha_i x alpha_j)
-// as alpha_i.(alpha_j x d) from the velocity's cross product, and the
-// diffusion as v_i sum(Dp alpha_j) - alpha_i sum(Dp v_j).  This is the
+// (pair_f32.cu): two rsqrt per pair, no pow, no division; alpha_i x alpha_j
+// per pair as the reference forms it, and the diffusion as
+// v_i sum(Dp alpha_j) - alpha_i sum(Dp v_j), taken after the pair loop.
+// (Forming the stretching's q-term as alpha_i x sum(q alpha_j) and the triple
+// product from the velocity's cross product as well saves six more operations
+// per pair but sums nearly parallel neighbours' terms coherently before the
+// cross product: 100 times the rounding error of the per-pair form.)  This is the
 // "tuned FP64" variant, reported beside the FP32 kernel and the plain FP64
 // comparator (pair_plain.cu).  Same work items, partial layout and gather form.
 //
@@ -74,9 +76,9 @@ __global__ void __launch_bounds__(TB)
       vi = sg.vor64[i];
     }
     const double hi = 0.5 * pi.w * pi.w;
-    // u = sum qh (alpha_j x d); Q = sum qh alpha_j (the q-term of the
-    // stretching is alpha_i x Q); G = sum fh [alpha_i.(alpha_j x d)] d;
-    // E = sum Dp alpha_j, V = sum Dp v_j (the diffusion is v_i E - V alpha_i)
+    // u = sum qh (alpha_j x d); q = sum qh (alpha_i x alpha_j);
+    // G = sum fh [d.(alpha_i x alpha_j)] d; E = sum Dp alpha_j, V = sum Dp v_j
+    // (the diffusion is v_i E - V alpha_i)
     double ux = 0, uy = 0, uz = 0, qx = 0, qy = 0, qz = 0, gx = 0, gy = 0, gz = 0;
     double ex = 0, ey = 0, ez = 0, ev = 0;
 
@@ -116,12 +118,13 @@ __global__ void __launch_bounds__(TB)
           qh = fma(-7.5, zc, ph) * sig2 * ri2;
           fh = fma(2.5, zc, -qh) * ri2;
         }
-        // alpha_j x d, for the velocity and (dotted with alpha_i) for the
-        // triple product d.(alpha_i x alpha_j) = alpha_i.(alpha_j x d)
         const double cx = fma(s.y, dz, -s.z * dy);
         const double cy = fma(s.z, dx, -s.x * dz);
         const double cz = fma(s.x, dy, -s.y * dx);
-        const double tt = fma(vi.z, cz, fma(vi.y, cy, vi.x * cx));
+        const double wx = fma(vi.y, s.z, -vi.z * s.y);
+        const double wy = fma(vi.z, s.x, -vi.x * s.z);
+        const double wz = fma(vi.x, s.y, -vi.y * s.x);
+        const double tt = fma(dz, wz, fma(dy, wy, dx * wx));
         double ft = fh * tt;
         const bool self = (jj == skip);
         qh = self ? 0.0 : qh;
@@ -130,9 +133,9 @@ __global__ void __launch_bounds__(TB)
         ux = fma(qh, cx, ux);
         uy = fma(qh, cy, uy);
         uz = fma(qh, cz, uz);
-        qx = fma(qh, s.x, qx);
-        qy = fma(qh, s.y, qy);
-        qz = fma(qh, s.z, qz);
+        qx = fma(qh, wx, qx);
+        qy = fma(qh, wy, qy);
+        qz = fma(qh, wz, qz);
         gx = fma(ft, dx, gx);
         gy = fma(ft, dy, gy);
         gz = fma(ft, dz, gz);
@@ -147,13 +150,9 @@ __global__ void __launch_bounds__(TB)
 
     if (valid) {
       const double A = kInv4Pi;
-      // alpha_i x Q
-      const double wx = fma(vi.y, qz, -vi.z * qy);
-      const double wy = fma(vi.z, qx, -vi.x * qz);
-      const double wz = fma(vi.x, qy, -vi.y * qx);
-      double dax = A * wx + 3.0 * A * gx;
-      double day = A * wy + 3.0 * A * gy;
-      double daz = A * wz + 3.0 * A * gz;
+      double dax = A * qx + 3.0 * A * gx;
+      double day = A * qy + 3.0 * A * gy;
+      double daz = A * qz + 3.0 * A * gz;
       if (DIFF) {
         // v_i E - V alpha_i
         const double c = 15.0 * sg.nu * A;
